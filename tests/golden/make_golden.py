@@ -1,0 +1,246 @@
+"""Generate golden vectors by running the jax-hfbfft reference modules themselves.
+
+JAX is not installed in the build container, so the reference modules are
+imported unmodified with ``tests/golden/jaxshim`` first on ``sys.path``: a
+NumPy-backed stand-in for the subset of the jax API they use (see the
+docstring of ``jaxshim/jax/__init__.py`` for the semantics restated).
+
+Run from the repository root, in the build container only (it reads the
+reference checkout)::
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+Outputs (committed): ``tests/golden/unit_n8.npz`` (per-function vectors on an
+8^3 grid with seeded random inputs) and ``tests/golden/run_<case>.npz``
+(end-to-end runs of the reference driver ``statichf_with_benchmark`` on small
+grids: per-iteration energies and final densities / levels).
+"""
+import argparse
+import contextlib
+import io
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+from cases import RUN_CASES  # noqa: E402  (shared with the tests)
+
+
+def _import_reference(ref):
+    sys.path.insert(0, os.path.join(HERE, "jaxshim"))
+    sys.path.insert(1, ref)
+    import jax  # noqa: F401  (the stand-in)
+    mods = {}
+    for name in ("params", "forces", "grids", "densities", "meanfield", "levels", "static",
+                 "coulomb", "moment", "energies", "pairs", "output", "inout", "trivial"):
+        mods[name] = __import__(name)
+    return mods
+
+
+def _setup(m, ref, case):
+    cwd = os.getcwd()
+    os.chdir(ref)      # forces.py reads _forces.yml relative to the working directory
+    try:
+        params = m["params"].init_params(imode=1, tfft=True, mprint=case.get("mprint", 1), nof=0)
+        forces = m["forces"].init_forces(params, **case["force"])
+    finally:
+        os.chdir(cwd)
+    grids = m["grids"].init_grids(params, **case["grid"])
+    dens = m["densities"].init_densities(grids)
+    mf = m["meanfield"].init_meanfield(grids)
+    levels = m["levels"].init_levels(grids, **case["levels"])
+    forces, static = m["static"].init_static(forces, levels, **case["static"])
+    coul = m["coulomb"].init_coulomb(grids)
+    en = m["energies"].init_energies()
+    moment = m["moment"].init_moment(np.array([0.0, 0.0, 0.0]))
+    pairs = m["pairs"].Pairs()
+    return params, forces, grids, dens, mf, levels, static, coul, en, moment, pairs
+
+
+def run_case(m, ref, name, case):
+    params, forces, grids, dens, mf, levels, static, coul, en, moment, pairs = _setup(m, ref, case)
+    levels = m["static"].harmosc(grids, levels, params, static)
+    psi0 = np.array(levels.psi)
+    hist = []
+    st_mod = m["static"]
+    orig_sum = st_mod.sum_energy
+
+    def recording_sum_energy(energies, lv, meanfield, pr):
+        e = orig_sum(energies, lv, meanfield, pr)
+        hist.append((params.iteration, float(e.ehf), float(e.ehfint), float(e.efluct1[0]), float(e.efluct2[0]),
+                     float(static.x0dmp), float(np.sum(pr.epair))))
+        return e
+
+    st_mod.sum_energy = recording_sum_energy
+    st_mod.lastdiag = lambda *a, **k: (np.zeros(0), np.zeros(0))   # post-loop printout only
+    tmp = tempfile.mkdtemp()
+    cwd = os.getcwd()
+    os.chdir(tmp)
+    try:
+        with contextlib.redirect_stdout(io.StringIO()):
+            out = st_mod.statichf_with_benchmark(coul, dens, en, forces, grids, levels, mf, moment, params,
+                                                 static, pairs, m["output"].FortranOutputWriter(tmp))
+    finally:
+        os.chdir(cwd)
+        st_mod.sum_energy = orig_sum
+    coul, dens, en, forces, grids, levels, mf = out[:7]
+    obs_mod = m["output"]
+    with contextlib.redirect_stdout(io.StringIO()):
+        obs = obs_mod.calculate_complete_observables(dens, levels, grids, params)
+    h = np.array(hist)
+    np.savez_compressed(
+        os.path.join(HERE, f"run_{name}.npz"),
+        hist_iter=h[:, 0], hist_ehf=h[:, 1], hist_ehfint=h[:, 2], hist_efluct1=h[:, 3],
+        hist_efluct2=h[:, 4], hist_x0dmp=h[:, 5], hist_epair=h[:, 6],
+        psi0=psi0,
+        rho=np.asarray(dens.rho), tau=np.asarray(dens.tau), chi=np.asarray(dens.chi),
+        sp_energy=np.asarray(levels.sp_energy), sp_kinetic=np.asarray(levels.sp_kinetic),
+        wocc=np.asarray(levels.wocc), wguv=np.asarray(levels.wguv), pairwg=np.asarray(levels.pairwg),
+        wstates=np.asarray(levels.wstates), deltaf=np.asarray(levels.deltaf),
+        eferm=np.asarray(pairs.eferm), epair=np.asarray(pairs.epair),
+        rms=np.asarray(obs.rms), rmstot=np.asarray(obs.rmstot),
+        ehf=float(en.ehf), ehfint=float(en.ehfint),
+        upot=np.asarray(mf.upot), wcoul=np.asarray(coul.wcoul))
+    print(f"{name}: {len(hist)} energy records, ehf={en.ehf:.10f}")
+
+
+def _smooth_random(rng, shape, n, scale):
+    """Seeded smooth random field: a few low Fourier modes, real."""
+    f = np.zeros(shape, dtype=np.complex128)
+    lead = shape[:-3]
+    for _ in range(6):
+        k = rng.integers(-2, 3, size=3)
+        amp = rng.normal(size=lead) + 1j * rng.normal(size=lead)
+        ph = np.exp(2j * np.pi * (k[0] * np.arange(n)[:, None, None] + k[1] * np.arange(n)[None, :, None]
+                                  + k[2] * np.arange(n)[None, None, :]) / n)
+        f = f + np.asarray(amp)[..., None, None, None] * ph
+    return scale * f.real
+
+
+def unit_vectors(m, ref):
+    """Per-function golden vectors on an 8^3 grid, dx=0.9, seeded inputs."""
+    rng = np.random.default_rng(20261203)
+    n = 8
+    case = dict(grid=dict(nx=n, ny=n, nz=n, dx=0.9, dy=0.9, dz=0.9),
+                force=dict(name="SLy4", ipair=6, tbcs=False, v0prot=362.0, v0neut=362.0, rho0pr=0.32),
+                levels=dict(nneut=3, nprot=2, npsi=[4, 3]),
+                static=dict(maxiter=1, radinx=2.0, radiny=2.1, radinz=2.4, serr=1e-20, x0dmp=0.3, e0dmp=100.0),
+                mprint=1)
+    params, forces, grids, dens, mf, levels, static, coul, en, moment, pairs = _setup(m, ref, case)
+    import jax.numpy as jnp  # the stand-in: arrays assigned into reference objects need ``.at``
+    J = jnp.asarray
+    lev = m["levels"]
+    out = {}
+    psi = rng.normal(size=(2, n, n, n)) + 1j * rng.normal(size=(2, n, n, n))
+    bfield = 20.0 + _smooth_random(rng, (n, n, n), n, 1.0)
+    out["in_psi"] = psi
+    out["in_b"] = bfield
+    for ax, tag in ((1, "x"), (2, "y"), (3, "z")):
+        out[f"cderv{tag}00"] = np.asarray(getattr(lev, f"cderv{tag}00")(0.9, psi))
+        d1, d2 = getattr(lev, f"cderv{tag}01")(0.9, psi)
+        out[f"cderv{tag}01_d1"], out[f"cderv{tag}01_d2"] = np.asarray(d1), np.asarray(d2)
+        d1, d2 = getattr(lev, f"cderv{tag}02")(0.9, psi, bfield)
+        out[f"cderv{tag}02_d1"], out[f"cderv{tag}02_d2"] = np.asarray(d1), np.asarray(d2)
+    out["laplace_bcs"] = np.asarray(lev.laplace(0, 0, grids, forces, levels, 1.0, 0.0, psi, 0.0, 100.0))
+    out["laplace_hfb"] = np.asarray(lev.laplace(0, 0, grids, forces, levels, 0.37, 0.02, psi, 3.5, 100.0))
+    # hpsi01 with seeded smooth potentials
+    s4 = (2, n, n, n)
+    s5 = (2, 3, n, n, n)
+    mf.upot = J(-50.0 + _smooth_random(rng, s4, n, 10.0))
+    mf.bmass = J(20.0 + _smooth_random(rng, s4, n, 2.0))
+    mf.v_pair = J(_smooth_random(rng, s4, n, 5.0))
+    mf.aq = J(_smooth_random(rng, s5, n, 1.0))
+    mf.spot = J(_smooth_random(rng, s5, n, 1.0))
+    mf.wlspot = J(_smooth_random(rng, s5, n, 3.0))
+    for k in ("upot", "bmass", "v_pair", "aq", "spot", "wlspot"):
+        out[f"in_mf_{k}"] = np.asarray(getattr(mf, k))
+    for iq in range(2):
+        po, pm, pd = m["meanfield"].hpsi01(grids, mf, iq, 0.8, 0.3, psi)
+        out[f"hpsi_iq{iq}_pout"], out[f"hpsi_iq{iq}_mf"], out[f"hpsi_iq{iq}_del"] = (
+            np.asarray(po), np.asarray(pm), np.asarray(pd))
+    # add_density on seeded states and weights
+    nst = levels.nstmax
+    levels.psi = J((rng.normal(size=(nst, 2, n, n, n)) + 1j * rng.normal(size=(nst, 2, n, n, n))) * 0.05)
+    levels.wocc = J(rng.uniform(0.0, 1.0, size=nst))
+    levels.wguv = J(rng.uniform(0.0, 0.5, size=nst))
+    levels.pairwg = J(rng.uniform(0.5, 1.0, size=nst))
+    levels.wstates = J(rng.uniform(0.8, 1.0, size=nst))
+    out["in_dens_psi"] = np.asarray(levels.psi)
+    for k in ("wocc", "wguv", "pairwg", "wstates"):
+        out[f"in_dens_{k}"] = np.asarray(getattr(levels, k))
+    d = m["densities"].add_density(dens, grids, levels)
+    for k in ("rho", "chi", "tau", "current", "sdens", "sodens"):
+        out[f"dens_{k}"] = np.asarray(getattr(d, k))
+    # skyrme on physical-looking densities (Gaussian rho/tau/chi plus the seeded vector fields)
+    x = np.asarray(grids.x)
+    r2 = x[:, None, None] ** 2 + x[None, :, None] ** 2 + (1.1 * x[None, None, :]) ** 2
+    d.rho = J(np.stack([0.08 * np.exp(-r2 / 6.0), 0.07 * np.exp(-r2 / 5.5)]))
+    d.tau = J(np.stack([0.1 * np.exp(-r2 / 5.0), 0.09 * np.exp(-r2 / 5.0)]))
+    d.chi = J(np.stack([0.01 * np.exp(-r2 / 7.0), 0.012 * np.exp(-r2 / 7.0)]))
+    for k in ("rho", "tau", "chi"):
+        out[f"in_sky_{k}"] = np.asarray(getattr(d, k))
+    with contextlib.redirect_stdout(io.StringIO()):
+        mf2, coul2 = m["meanfield"].skyrme(coul, d, forces, grids, mf, params, static)
+    for k in ("upot", "bmass", "divaq", "v_pair", "aq", "spot", "wlspot", "dbmass"):
+        out[f"sky_{k}"] = np.asarray(getattr(mf2, k))
+    out["sky_ecorrp"] = float(mf2.ecorrp)
+    out["sky_wcoul"] = np.asarray(coul2.wcoul)
+    out["coulomb_q"] = np.asarray(coul2.q)
+    # energies on the same densities and levels
+    levels.sp_energy = J(rng.uniform(-40.0, 5.0, size=nst))
+    levels.sp_kinetic = J(rng.uniform(5.0, 30.0, size=nst))
+    pairs.epair = J(np.array([1.3, 0.7]))
+    out["in_en_sp_energy"] = np.asarray(levels.sp_energy)
+    out["in_en_sp_kinetic"] = np.asarray(levels.sp_kinetic)
+    e = m["energies"].integ_energy(coul2, d, en, forces, grids, levels, params, pairs)
+    e = m["energies"].sum_energy(e, levels, mf2, pairs)
+    for k in ("ehft", "ehf0", "ehf1", "ehf2", "ehf3", "ehfls", "ehflsodd", "ehfc", "ecorc", "ehfint",
+              "e3corr", "ehf", "tke", "ehfCrho0", "ehfCrho1", "ehfCdrho0", "ehfCdrho1", "ehfCtau0",
+              "ehfCtau1", "ehfCdJ0", "ehfCdJ1"):
+        out[f"en_{k}"] = float(getattr(e, k))
+    # sp_properties
+    lv = m["inout"].sp_properties(forces, grids, levels, moment)
+    for k in ("sp_kinetic", "sp_spin", "sp_orbital", "sp_parity"):
+        out[f"spp_{k}"] = np.asarray(getattr(lv, k))
+    # BCS on synthetic spectra
+    levels.sp_energy = J(np.sort(rng.uniform(-30.0, 10.0, size=nst)))
+    levels.deltaf = J(rng.uniform(0.5, 2.0, size=nst))
+    levels.wstates = J(np.ones(nst))
+    levels.pairwg = J(np.ones(nst))
+    out["in_bcs_sp_energy"] = np.asarray(levels.sp_energy)
+    out["in_bcs_deltaf"] = np.asarray(levels.deltaf)
+    params.iteration = 11
+    forces.pair_cutoff = J(np.array([5.0, 5.0]))
+    forces.state_cutoff = J(np.array([20.0, 20.0]))
+    pr = m["pairs"].Pairs()
+    pr.firstcall = False
+    with contextlib.redirect_stdout(io.StringIO()):
+        lv, pr = m["pairs"].pair(levels, mf2, forces, params, grids, pr)
+    for k in ("wocc", "wguv", "pairwg", "wstates", "deltaf"):
+        out[f"bcs_{k}"] = np.asarray(getattr(lv, k))
+    for k in ("eferm", "epair", "avdelt", "avdeltv2", "avg"):
+        out[f"bcs_{k}"] = np.asarray(getattr(pr, k))
+    np.savez_compressed(os.path.join(HERE, "unit_n8.npz"), **out)
+    print(f"unit_n8: {len(out)} arrays")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    m = _import_reference(a.ref)
+    if a.only in (None, "unit"):
+        unit_vectors(m, a.ref)
+    for name, case in RUN_CASES.items():
+        if a.only in (None, name):
+            m = _import_reference(a.ref)
+            run_case(m, a.ref, name, case)
+
+
+if __name__ == "__main__":
+    main()
