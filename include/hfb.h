@@ -1,0 +1,237 @@
+/*
+ * hfb.h -- C ABI of libhfb, the B200 (sm_100a) implementation of the static
+ * Skyrme HF+BCS iteration of jax-hfbfft.
+ *
+ * Every entry point takes plain device pointers, sizes and scalars, and a
+ * CUDA stream (cudaStream_t passed as void*; NULL = legacy default stream).
+ * Work is enqueued asynchronously; the return value is an hfb_status for the
+ * launch itself.  Errors detected on the device (a Fermi level that is not
+ * bracketed, a Jacobi sweep limit, a non-finite energy) are latched in the
+ * context and read with hfb_device_status(), which synchronises the stream.
+ *
+ * Layouts (identical to the reference's arrays, C order):
+ *   psi      [nst][2][nx][ny][nz]   complex (interleaved re,im), complex128
+ *                                   for HFB_F64, complex64 for HFB_F32;
+ *                                   neutron states first (levels.py:54)
+ *   fields   [2][nx][ny][nz]        double   (rho, tau, chi, upot, ...)
+ *   vectors  [2][3][nx][ny][nz]     double   (current, sdens, sodens, aq, ...)
+ *   pot      [2][12][nx][ny][nz]    real of the precision: upot, bmass,
+ *                                   v_pair, aq_xyz, spot_xyz, wlspot_xyz
+ *                                   (written by hfb_skyrme, read by hfb_hpsi)
+ *   matrices [2][nmax][nmax]        complex128, nmax = max(npsi)
+ *
+ * Grids must be cubic (nx == ny == nz) with n in {8, 16, 24, 32, 40, 48};
+ * spacings may differ per axis.
+ */
+#ifndef HFB_H
+#define HFB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hfb_ctx_s* hfb_ctx_t;
+
+enum hfb_status {
+  HFB_OK = 0,
+  HFB_ERR_ARG = 1,              /* bad argument / null pointer           */
+  HFB_ERR_UNSUPPORTED_GRID = 2, /* grid size not compiled in             */
+  HFB_ERR_CUDA = 3,             /* CUDA launch or runtime error          */
+  HFB_ERR_NOT_BRACKETED = 4,    /* BCS particle number not bracketed on
+                                   [-100, 100] (pairs.py:59 raises)      */
+  HFB_ERR_NO_CONVERGENCE = 5,   /* Jacobi or Brent iteration limit       */
+  HFB_ERR_NONFINITE = 6,        /* NaN / Inf in an energy or a norm      */
+  HFB_ERR_ALLOC = 7             /* device allocation failed              */
+};
+
+enum hfb_precision { HFB_F64 = 0, HFB_F32 = 1 };
+
+/* Skyrme force and pairing parameters; the derived b/C coefficients follow
+ * forces.py:95-122 and are filled by the host (see hfb/forces.py). */
+typedef struct hfb_force {
+  double b0, b0p, b1, b1p, b2, b2p, b3, b3p, b4, b4p, power, slate;
+  double h2m[2];           /* after the (A-1)/A scaling of static.py:87-88 */
+  double h2ma;             /* unscaled 0.5*(h2m_n+h2m_p), forces.py:141   */
+  double v0neut, v0prot, rho0pr;
+  double Crho0, Crho1, Crho0D, Crho1D, Cdrho0, Cdrho1, Ctau0, Ctau1, CdJ0, CdJ1;
+  int ipair;               /* 0 none, 5 VDI, 6 DDDI                        */
+  int ex;                  /* Slater exchange on/off                        */
+  int zpe;                 /* 1: c.m. correction 17.3/A^0.2                 */
+  int pad_;
+} hfb_force;
+
+/* ---- set-up ------------------------------------------------------------ */
+/* grids.py:66-138, coulomb.py:23-52: grid, dense derivative matrices and the
+ * doubled-grid Coulomb Green's function (built on the device).  nstmax sizes
+ * the scratch arena. */
+int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, double dz, int periodic,
+                   int nstmax, hfb_ctx_t* out);
+int hfb_ctx_destroy(hfb_ctx_t ctx);
+const char* hfb_status_string(int status);
+/* Latched device-side status (synchronises the stream), then clears it. */
+int hfb_device_status(hfb_ctx_t ctx, void* stream, int* status_out);
+
+/* ---- levels.py --------------------------------------------------------- */
+/* cderv{x,y,z}00 / 01 / 02 (levels.py:132-395) on nsp spinors.
+ * kind 0: d1 only; 1: d1 and d2 (Nyquist kept); 2: d1 and d(B d1) with the
+ * mean-B Nyquist term; axis 0,1,2 = x,y,z; bfield [nx][ny][nz] (kind 2). */
+int hfb_cderv(hfb_ctx_t ctx, int prec, int kind, int axis, int nsp, const void* psin,
+              const double* bfield, void* d1, void* d2, void* stream);
+/* laplace (levels.py:398-437) on nsp spinors with per-spinor weights
+ * wg[nsp], wguv[nsp]; v_pairmax scalar; e0inv = static.e0dmp. */
+int hfb_laplace(hfb_ctx_t ctx, int prec, int nsp, const void* psin, const double* wg,
+                const double* wguv, double v_pairmax, double e0inv, double h2ma, void* psout,
+                void* stream);
+
+/* ---- meanfield.py ------------------------------------------------------ */
+/* hpsi01 (meanfield.py:41-159) batched over nst states; state s uses the
+ * potentials of isospin (s >= nneut).  Any of pout / pout_mf / pout_del may
+ * be NULL except that one of pout / pout_mf is required. */
+int hfb_hpsi(hfb_ctx_t ctx, int prec, const void* pot, int nst, int nneut, const void* psi,
+             const double* weight, const double* weightuv, void* pout, void* pout_mf,
+             void* pout_del, void* stream);
+/* skyrme (meanfield.py:164-391): all mean fields from the densities, the
+ * Coulomb potential (if tcoul) and ecorrp (device scalar); also packs the
+ * hpsi potentials into pot (precision prec). */
+int hfb_skyrme(hfb_ctx_t ctx, const hfb_force* f, int tcoul, const double* rho, const double* tau,
+               const double* chi, const double* current, const double* sdens, const double* sodens,
+               double* upot, double* bmass, double* divaq, double* v_pair, double* aq, double* spot,
+               double* wlspot, double* dbmass, double* wcoul, double* ecorrp, int prec, void* pot,
+               void* stream);
+
+/* ---- coulomb.py -------------------------------------------------------- */
+/* poisson (coulomb.py:54-75): wcoul[nx][ny][nz] from the proton density. */
+int hfb_poisson(hfb_ctx_t ctx, const double* rho_p, double* wcoul, void* stream);
+
+/* ---- densities.py / inout.py ------------------------------------------- */
+/* add_density (densities.py:177-234) over nst states (neutrons first).
+ * If mix < 1, rho/tau/chi are blended as mix*new + (1-mix)*old in place
+ * (static.py:1820-1823); current/sdens/sodens are always replaced.
+ * sp_kinetic (optional, may be NULL) receives the per-state kinetic energy
+ * of inout.py:129-132, computed from the same derivatives; h2m is a HOST
+ * array of 2 doubles (neutron, proton). */
+int hfb_add_density(hfb_ctx_t ctx, int prec, int nst, int nneut, const void* psi,
+                    const double* wocc, const double* wguv, const double* pairwg,
+                    const double* wstates, double mix, double* rho, double* chi, double* tau,
+                    double* current, double* sdens, double* sodens, const double* h2m,
+                    double* sp_kinetic, void* stream);
+/* sp_properties kinetic part alone (inout.py:64-150); h2m host array [2]. */
+int hfb_sp_kinetic(hfb_ctx_t ctx, int prec, int nst, int nneut, const void* psi,
+                   const double* h2m, double* sp_kinetic, void* stream);
+
+/* ---- static.py --------------------------------------------------------- */
+/* harmosc (static.py:580-738): state s = Gaussian * x^i y^j z^k in spin
+ * component c, normalised; qn is a DEVICE int array [nst][4] = (i, j, k, c).
+ */
+int hfb_harmosc(hfb_ctx_t ctx, int prec, int nst, const int* qn, double radinx, double radiny,
+                double radinz, void* psi, void* stream);
+
+typedef struct hfb_grstep_args {
+  int nst, nneut;
+  int tbcs;                /* forces.tbcs                                     */
+  int use_lagrange;        /* (iteration > 1) and not tbcs  (static.py:99)   */
+  int do_fluct;            /* mprint > 0 and iteration % mprint == 0         */
+  int pad_;
+  double x0dmp, e0dmp, h2ma, wxyz;
+  const void* pot;         /* packed potentials [2][12][N]                    */
+  const double* v_pair;    /* [2][N] double, for max(v_pair[iq])              */
+  void* psi;               /* in/out                                         */
+  void* hampsi;            /* out: h psi_old (unweighted)                    */
+  void* hmfpsi;            /* out: h psi_new (unweighted); scratch before    */
+  void* delpsi;            /* out (optional): v_pair psi_new                 */
+  const void* lagrange;
+  const double *wocc, *wguv, *pairwg, *wstates;
+  double* sp_energy;       /* in: previous; out: <psi_old|h|psi_old>         */
+  double* sp_efluct1;      /* in/out                                         */
+  double* sp_efluct2;      /* in/out                                         */
+  double* sums;            /* out [2]: sum(sp_efluct1), sum(wocc*wstates*denerg) */
+} hfb_grstep_args;
+/* grstep (static.py:215-259) with grstep_helper / e0dmp_gt_zero / laplace. */
+int hfb_grstep(hfb_ctx_t ctx, int prec, const hfb_grstep_args* a, void* stream);
+
+typedef struct hfb_diag_args {
+  int npsi[2];
+  int nmax;                /* leading dimension of the matrices              */
+  int diagonalize;         /* eigh of lambda (static.py:300-303)             */
+  int construct;           /* construct_hfb_matrices vs lagrange update      */
+  int ipair, tbcs, pad_;
+  double wxyz;
+  const void* psi;         /* in: states after the gradient step             */
+  void* psi_out;           /* out: rotated states psi U (must not alias psi) */
+  const void* hampsi;
+  const void* hmfpsi;
+  void* lagrange;          /* out                                            */
+  const double* v_pair;    /* [2][N], delpsi = v_pair * psi_new (static.py:203) */
+  const double *wocc, *wguv, *pairwg, *wstates;
+  double* sp_norm;         /* out                                            */
+  double* sp_energy;       /* out (construct)                                */
+  double* deltaf;          /* out (construct, ipair != 0)                    */
+  double* hmatrix;         /* complex [2][nmax][nmax]                        */
+  double* gapmatrix;
+  double* symcond;
+  double* lambda_save;     /* in (construct == 0) / out                      */
+  double* efluct;          /* out [4]: efluct1q[2], efluct2q[2]              */
+} hfb_diag_args;
+/* diagstep (static.py:261-461) with loewdin_orthonormalize (463-482) and
+ * construct_hfb_matrices (484-577).  Works on both isospins (npsi[0]
+ * neutron states first); each isospin block must have at most 166 states
+ * (the Jacobi solver holds the packed matrix in one CTA's shared memory). */
+int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, void* stream);
+
+/* Building blocks of diagstep, exported for tests:
+ * C_a = wxyz * Psi^H X_a for a in the mask (bit0 X=psi, bit1 X=hampsi,
+ * bit2 X=hmfpsi, bit3 X=v_pair*psi), states [s0, s0+ns), out complex
+ * [4][ns][ns]. */
+int hfb_gram(hfb_ctx_t ctx, int prec, int s0, int ns, int mask, const void* psi,
+             const void* hampsi, const void* hmfpsi, const double* v_pair_iq, double wxyz,
+             double* out, void* stream);
+/* Hermitian eigensolver (cyclic Jacobi, FP64) on nb matrices a[nb][n][lda]
+ * using their lower triangle; eigenvalues ascending in w[nb][n],
+ * eigenvectors in the columns of v[nb][n][lda]. */
+int hfb_eigh(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w, double* v,
+             void* stream);
+
+/* ---- pairs.py ---------------------------------------------------------- */
+typedef struct hfb_pair_args {
+  int npsi[2];
+  int nneut, nprot;        /* particle numbers                               */
+  int use_const_gap;       /* iteration <= 10 (pairs.py:135)                 */
+  int pad_;
+  double const_gap;        /* 11.2 / sqrt(A)                                  */
+  double pair_cutoff[2], state_cutoff[2], softcut_range;
+  const double* sp_energy;
+  double *deltaf, *wocc, *wguv, *pairwg, *wstates;   /* in/out */
+  double* out;             /* [5][2]: eferm, epair, avdelt, avdeltv2, avg     */
+} hfb_pair_args;
+/* pair (pairs.py:161-220): gap, Fermi level by Brent's method on [-100,100]
+ * with xtol 1e-14 (pairs.py:59), soft cutoffs, v^2, uv and sums. */
+int hfb_pair(hfb_ctx_t ctx, const hfb_pair_args* a, void* stream);
+
+/* ---- energies.py / output.py ------------------------------------------- */
+/* integ_energy (energies.py:90-306).  out (device) receives HFB_NE doubles
+ * in the order of the HFB_E_* indices below (EHF and TKE are left for
+ * hfb_sum_energy). */
+enum {
+  HFB_E_EHFT = 0, HFB_E_EHF0, HFB_E_EHF1, HFB_E_EHF2, HFB_E_EHF3, HFB_E_EHFLS, HFB_E_EHFLSODD,
+  HFB_E_EHFC, HFB_E_ECORC, HFB_E_EHFINT, HFB_E_E3CORR, HFB_E_EZPE, HFB_E_EHF, HFB_E_TKE,
+  HFB_E_CRHO0, HFB_E_CRHO1, HFB_E_CDRHO0, HFB_E_CDRHO1, HFB_E_CTAU0, HFB_E_CTAU1, HFB_E_CDJ0,
+  HFB_E_CDJ1, HFB_E_CJ0, HFB_E_CJ1, HFB_NE
+};
+int hfb_energies(hfb_ctx_t ctx, const hfb_force* f, int tcoul, double mass_number,
+                 const double* rho, const double* tau, const double* current,
+                 const double* sdens, const double* sodens, const double* wcoul,
+                 const double* epair, double* out, void* stream);
+/* sum_energy (energies.py:309-372): out[HFB_E_EHF], out[HFB_E_TKE] from the
+ * single-particle sums and out[E3CORR, ECORC, EZPE] of hfb_energies; epair
+ * [2] and ecorrp [1] are device arrays. */
+int hfb_sum_energy(hfb_ctx_t ctx, int nst, const double* wocc, const double* wstates,
+                   const double* sp_kinetic, const double* sp_energy, const double* epair,
+                   const double* ecorrp, double* out, void* stream);
+/* Point rms radii (output.py:187-226, 246): out[0..1] particle numbers,
+ * out[2..3] rms per isospin, out[4] total rms. */
+int hfb_rms(hfb_ctx_t ctx, const double* rho, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HFB_H */

@@ -1,0 +1,150 @@
+// Context creation: grid, dense derivative matrices, Coulomb Green's
+// function, scratch arena and the device status latch.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+#include "hfb_ctx.cuh"
+
+namespace hfb {
+
+int coulomb_init(hfb_ctx_s* c);  // skyrme.cu
+
+void* scratch(hfb_ctx_s* c, int s, size_t bytes) {
+  if (s < 0 || s >= hfb_ctx_s::S_NSLOT) return nullptr;
+  if (bytes == 0) bytes = 16;
+  if (c->slot_bytes[s] >= bytes) return c->slot[s];
+  if (c->slot[s]) {
+    cudaDeviceSynchronize();
+    cudaFree(c->slot[s]);
+    c->slot[s] = nullptr;
+    c->slot_bytes[s] = 0;
+  }
+  size_t want = bytes + bytes / 8;
+  if (cudaMalloc(&c->slot[s], want) != cudaSuccess) {
+    cudaGetLastError();
+    c->slot[s] = nullptr;
+    return nullptr;
+  }
+  c->slot_bytes[s] = want;
+  return c->slot[s];
+}
+
+// Dense spectral derivative matrices, restating grids.py:36-61:
+//   der1[a][b] = afac/(icn d) sum_{j=1}^{icn-1} j sin(j afac (b-a))
+//                (the icn term vanishes: sin(pi (b-a)) = 0 in the reference's
+//                 arithmetic up to rounding, kept for identical rounding)
+//   der2[a][b] = -afac^2/(icn d^2) [sum_j j^2 cos(j afac (b-a)) + icn^2/2 cos(icn afac (b-a))]
+static void dense_derivatives(int n, double d, std::vector<double>& d1, std::vector<double>& d2) {
+  const int icn = (n + 1) / 2;
+  const double afac = M_PI / icn;
+  d1.assign((size_t)n * n, 0.0);
+  d2.assign((size_t)n * n, 0.0);
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b) {
+      const double g = (double)(b - a);
+      double s1 = 0.0, s2 = 0.0;
+      for (int j = 1; j < icn; ++j) {
+        s1 += -j * sin(j * afac * g);
+        s2 += (double)j * j * cos(j * afac * g);
+      }
+      d1[(size_t)a * n + b] = -afac * (s1 - 0.5 * icn * sin(icn * afac * g)) / (icn * d);
+      d2[(size_t)a * n + b] = -(afac * afac) * (s2 + 0.5 * icn * icn * cos(icn * afac * g)) / (icn * d * d);
+    }
+}
+
+}  // namespace hfb
+
+using namespace hfb;
+
+extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, double dz, int periodic, int nstmax,
+                              hfb_ctx_t* out) {
+  if (!out) return HFB_ERR_ARG;
+  *out = nullptr;
+  if (nx != ny || ny != nz) return HFB_ERR_UNSUPPORTED_GRID;
+  if (nx % 2 != 0) return HFB_ERR_ARG;        // grids.py:103-106
+  if (dx * dy * dz <= 0.0) {                  // grids.py:108-113
+    if (dx <= 0.0) return HFB_ERR_ARG;
+    dy = dz = dx;
+  }
+  int ok = dispatch_n(nx, [](auto) { return HFB_OK; });
+  if (ok != HFB_OK) return ok;
+  hfb_ctx_s* c = (hfb_ctx_s*)calloc(1, sizeof(hfb_ctx_s));
+  if (!c) return HFB_ERR_ALLOC;
+  c->n = nx;
+  c->d[0] = dx; c->d[1] = dy; c->d[2] = dz;
+  c->wxyz = dx * dy * dz;
+  c->periodic = periodic ? 1 : 0;
+  c->nstmax = nstmax;
+  c->n2 = periodic ? nx : 2 * nx;
+  const size_t nn = (size_t)nx * nx;
+  for (int a = 0; a < 3; ++a) {
+    std::vector<double> d1, d2;
+    dense_derivatives(nx, c->d[a], d1, d2);
+    if (cudaMalloc(&c->der1[a], nn * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->der2[a], nn * sizeof(double)) != cudaSuccess) {
+      hfb_ctx_destroy(c);
+      return HFB_ERR_ALLOC;
+    }
+    cudaMemcpy(c->der1[a], d1.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->der2[a], d2.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  if (cudaMalloc(&c->dev_status, sizeof(int)) != cudaSuccess) {
+    hfb_ctx_destroy(c);
+    return HFB_ERR_ALLOC;
+  }
+  cudaMemset(c->dev_status, 0, sizeof(int));
+  const size_t n2c = (size_t)c->n2 * c->n2 * c->n2;
+  if (cudaMalloc(&c->coul_q, n2c * sizeof(double2)) != cudaSuccess) {
+    hfb_ctx_destroy(c);
+    return HFB_ERR_ALLOC;
+  }
+  int r = coulomb_init(c);
+  if (r == HFB_OK && cudaDeviceSynchronize() != cudaSuccess) r = HFB_ERR_CUDA;
+  if (r != HFB_OK) {
+    hfb_ctx_destroy(c);
+    return r;
+  }
+  *out = c;
+  return HFB_OK;
+}
+
+extern "C" int hfb_ctx_destroy(hfb_ctx_t c) {
+  if (!c) return HFB_OK;
+  cudaDeviceSynchronize();
+  for (int a = 0; a < 3; ++a) {
+    if (c->der1[a]) cudaFree(c->der1[a]);
+    if (c->der2[a]) cudaFree(c->der2[a]);
+  }
+  if (c->coul_q) cudaFree(c->coul_q);
+  if (c->dev_status) cudaFree(c->dev_status);
+  for (int s = 0; s < hfb_ctx_s::S_NSLOT; ++s)
+    if (c->slot[s]) cudaFree(c->slot[s]);
+  free(c);
+  return HFB_OK;
+}
+
+extern "C" const char* hfb_status_string(int s) {
+  switch (s) {
+    case HFB_OK: return "ok";
+    case HFB_ERR_ARG: return "invalid argument";
+    case HFB_ERR_UNSUPPORTED_GRID: return "unsupported grid (cubic n in {8,16,24,32,40,48})";
+    case HFB_ERR_CUDA: return "CUDA error";
+    case HFB_ERR_NOT_BRACKETED: return "BCS particle number not bracketed on [-100, 100]";
+    case HFB_ERR_NO_CONVERGENCE: return "iteration limit reached (Jacobi / Brent)";
+    case HFB_ERR_NONFINITE: return "non-finite value";
+    case HFB_ERR_ALLOC: return "device allocation failed";
+    default: return "unknown status";
+  }
+}
+
+extern "C" int hfb_device_status(hfb_ctx_t c, void* stream, int* status_out) {
+  if (!c || !status_out) return HFB_ERR_ARG;
+  int h = 0;
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemcpyAsync(&h, c->dev_status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return HFB_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return HFB_ERR_CUDA;
+  if (h) cudaMemsetAsync(c->dev_status, 0, sizeof(int), st);
+  *status_out = h;
+  return HFB_OK;
+}

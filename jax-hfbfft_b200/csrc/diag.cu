@@ -1,0 +1,712 @@
+// Diagonalisation step: diagstep (static.py:261-461), loewdin_orthonormalize
+// (463-482) and construct_hfb_matrices (484-577).
+//
+//  * Gram contractions C_a = wxyz Psi^H X_a (X = psi, hampsi, hmfpsi,
+//    v_pair psi) over K = 2 n^3: one kernel reads each psi tile once for all
+//    requested matrices; split-K partials are summed in a fixed order.
+//  * Hermitian eigensolver: cyclic two-sided Jacobi in one CTA on the packed
+//    lower triangle held in shared memory (round-robin ordering, n/2 disjoint
+//    rotations per round); the rotations are recorded and replayed onto the
+//    eigenvector matrix by a row-parallel kernel.  Eigenvalues ascending.
+//  * small FP64 complex GEMMs for U = S^-1/2 V_lambda, U^H H U, U lambda.
+//  * rotation [psi_new | lagrange] = psi [U | U lambda_sym] as one GEMM pass.
+#include <math.h>
+#include "hfb_ctx.cuh"
+
+namespace hfb {
+
+// ================================================================ Gram ====
+constexpr int GT = 32;     // states per tile (both i and j)
+constexpr int GK = 16;     // k step staged in shared memory
+constexpr int GCHUNK = 8192;  // k per split-K chunk
+
+// part[chunk][a][i][j] (complex, unscaled); grid (tiles_i*tiles_j, nchunk)
+template <class R>
+__global__ void __launch_bounds__(256)
+gram_kernel(int ns, int mask, size_t K, size_t n3, const cplx<R>* __restrict__ psi, const cplx<R>* __restrict__ hampsi,
+            const cplx<R>* __restrict__ hmfpsi, const double* __restrict__ vp, double2* part) {
+  using Z = cplx<R>;
+  __shared__ Z As[GK][GT + 1];
+  __shared__ Z Bs[4][GK][GT + 1];
+  const int ntj = (ns + GT - 1) / GT;
+  const int ti = blockIdx.x / ntj, tj = blockIdx.x % ntj;
+  const int i0 = ti * GT, j0 = tj * GT;
+  const size_t k0 = (size_t)blockIdx.y * GCHUNK;
+  const size_t k1 = min(K, k0 + GCHUNK);
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;   // 16 x 16 threads, 2 x 2 outputs each
+  R acc[4][2][2][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) acc[a][u][v][0] = acc[a][u][v][1] = R(0);
+  const Z* X[3] = {psi, hampsi, hmfpsi};
+  for (size_t kb = k0; kb < k1; kb += GK) {
+    // stage: each thread loads 2 elements per operand (32 states x 16 k = 512)
+    for (int e = threadIdx.x; e < GT * GK; e += 256) {
+      const int s = e / GK, kk = e % GK;
+      const size_t k = kb + kk;
+      const bool ok_k = k < k1;
+      const int gi = i0 + s, gj = j0 + s;
+      As[kk][s] = (ok_k && gi < ns) ? psi[(size_t)gi * K + k] : czero<Z>();
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (!(mask & (1 << a))) continue;
+        Z v = czero<Z>();
+        if (ok_k && gj < ns) {
+          if (a < 3) v = X[a][(size_t)gj * K + k];
+          else v = (R)vp[k % n3] * psi[(size_t)gj * K + k];
+        }
+        Bs[a][kk][s] = v;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GK; ++kk) {
+      Z av[2];
+      av[0] = As[kk][ty];
+      av[1] = As[kk][ty + 16];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (!(mask & (1 << a))) continue;
+        Z bv0 = Bs[a][kk][tx], bv1 = Bs[a][kk][tx + 16];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          // conj(a) * b
+          acc[a][u][0][0] += av[u].x * bv0.x + av[u].y * bv0.y;
+          acc[a][u][0][1] += av[u].x * bv0.y - av[u].y * bv0.x;
+          acc[a][u][1][0] += av[u].x * bv1.x + av[u].y * bv1.y;
+          acc[a][u][1][1] += av[u].x * bv1.y - av[u].y * bv1.x;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const size_t stride = (size_t)ns * ns;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    if (!(mask & (1 << a))) continue;
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int gi = i0 + ty + 16 * u, gj = j0 + tx + 16 * v;
+        if (gi < ns && gj < ns)
+          part[((size_t)blockIdx.y * 4 + a) * stride + (size_t)gi * ns + gj] =
+              make_double2((double)acc[a][u][v][0], (double)acc[a][u][v][1]);
+      }
+  }
+}
+
+// out[a][i][j] (ld = ldo) = scale * sum_chunks part
+__global__ void gram_reduce_kernel(int ns, int mask, int nchunk, const double2* part, double scale, double2* out,
+                                   int ldo) {
+  const size_t stride = (size_t)ns * ns;
+  const size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int a = blockIdx.y;
+  if (e >= stride || !(mask & (1 << a))) return;
+  double re = 0, im = 0;
+  for (int c = 0; c < nchunk; ++c) {
+    double2 v = part[((size_t)c * 4 + a) * stride + e];
+    re += v.x;
+    im += v.y;
+  }
+  const int i = (int)(e / ns), j = (int)(e % ns);
+  out[(size_t)a * ldo * ldo + (size_t)i * ldo + j] = make_double2(scale * re, scale * im);
+}
+
+int gram_launch(hfb_ctx_s* c, int prec, int s0, int ns, int mask, const void* psi, const void* hampsi,
+                const void* hmfpsi, const double* vp, double wxyz, double2* out, int ldo, cudaStream_t st) {
+  if (ns <= 0 || mask == 0) return HFB_OK;
+  const size_t n3 = (size_t)c->n * c->n * c->n, K = 2 * n3;
+  const int nchunk = (int)((K + GCHUNK - 1) / GCHUNK);
+  const int nt = (ns + GT - 1) / GT;
+  double2* part = (double2*)scratch(c, hfb_ctx_s::S_GRAM, sizeof(double2) * (size_t)nchunk * 4 * ns * ns);
+  if (!part) return HFB_ERR_ALLOC;
+  dim3 grid(nt * nt, nchunk);
+  const size_t off = (size_t)s0 * K;
+  if (prec == HFB_F64)
+    gram_kernel<double><<<grid, 256, 0, st>>>(ns, mask, K, n3, (const double2*)psi + off,
+                                              hampsi ? (const double2*)hampsi + off : nullptr,
+                                              hmfpsi ? (const double2*)hmfpsi + off : nullptr, vp, part);
+  else
+    gram_kernel<float><<<grid, 256, 0, st>>>(ns, mask, K, n3, (const float2*)psi + off,
+                                             hampsi ? (const float2*)hampsi + off : nullptr,
+                                             hmfpsi ? (const float2*)hmfpsi + off : nullptr, vp, part);
+  HFB_CHECK_LAUNCH();
+  dim3 g2((unsigned)(((size_t)ns * ns + 255) / 256), 4);
+  gram_reduce_kernel<<<g2, 256, 0, st>>>(ns, mask, nchunk, part, wxyz, out, ldo);
+  HFB_CHECK_LAUNCH();
+  return HFB_OK;
+}
+
+// ============================================================== Jacobi ====
+// Packed lower triangle: element (k, l), k >= l, at k (k + 1) / 2 + l.
+__device__ __forceinline__ int pk(int k, int l) { return k * (k + 1) / 2 + l; }
+__device__ __forceinline__ double2 ld_h(const double2* a, int k, int l) {
+  if (k >= l) return a[pk(k, l)];
+  double2 v = a[pk(l, k)];
+  return make_double2(v.x, -v.y);
+}
+__device__ __forceinline__ void st_h(double2* a, int k, int l, double2 v) {
+  if (k >= l) a[pk(k, l)] = v;
+  else a[pk(l, k)] = make_double2(v.x, -v.y);
+}
+
+// Round-robin tournament: round r of m-1 (m even), pair index q < m/2.
+__device__ __forceinline__ void rr_pair(int m, int r, int q, int& a, int& b) {
+  if (q == 0) { a = r % (m - 1); b = m - 1; }
+  else { a = (r + q) % (m - 1); b = (r + m - 1 - q) % (m - 1); }
+  if (a > b) { int t = a; a = b; b = t; }
+}
+
+struct Pair2 {
+  int v[2];
+};
+
+struct JacRot {
+  double cs, sn;
+  double2 om;   // exp(-i phi)
+};
+
+constexpr int kJacMaxSweeps = 40;
+
+// One CTA per matrix.  ``rot`` receives the rotations
+// [sweep][round][m/2]; ``nrounds_out`` the number of recorded rounds.
+__global__ void __launch_bounds__(1024)
+jacobi_kernel(int n, int lda, const double2* __restrict__ A, double* w, JacRot* rot, int* nrounds_out, int* status,
+              size_t rot_stride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int b = blockIdx.x;
+  const int m = n + (n & 1);   // pad odd sizes with a decoupled index
+  double2* a = reinterpret_cast<double2*>(smem_raw);
+  JacRot* rr = reinterpret_cast<JacRot*>(a + (size_t)m * (m + 1) / 2);
+  __shared__ int any_rot;
+  const double2* Ab = A + (size_t)b * n * lda;
+  JacRot* rotb = rot + (size_t)b * rot_stride;
+  // load the lower triangle (eigh with symmetrize_input=False reads only it;
+  // the diagonal's imaginary part is ignored as by LAPACK zheevd)
+  for (int e = threadIdx.x; e < m * (m + 1) / 2; e += blockDim.x) {
+    int k = (int)((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
+    while (k * (k + 1) / 2 > e) --k;
+    while ((k + 1) * (k + 2) / 2 <= e) ++k;
+    const int l = e - k * (k + 1) / 2;
+    double2 v = make_double2(0.0, 0.0);
+    if (k < n && l < n) v = Ab[(size_t)k * lda + l];
+    if (k == l) v.y = 0.0;
+    a[e] = v;
+  }
+  __syncthreads();
+  const int half = m / 2;
+  int rounds = 0;
+  int sweep = 0;
+  for (; sweep < kJacMaxSweeps; ++sweep) {
+    if (threadIdx.x == 0) any_rot = 0;
+    __syncthreads();
+    for (int r = 0; r < m - 1; ++r) {
+      // rotation parameters for each disjoint pair
+      for (int q = threadIdx.x; q < half; q += blockDim.x) {
+        int p_, q_;
+        rr_pair(m, r, q, p_, q_);
+        JacRot g;
+        g.cs = 1.0; g.sn = 0.0; g.om = make_double2(1.0, 0.0);
+        const double app = a[pk(p_, p_)].x, aqq = a[pk(q_, q_)].x;
+        const double2 apq = ld_h(a, p_, q_);
+        const double mag = hypot(apq.x, apq.y);
+        // negligible off-diagonal element: relative to both diagonal entries
+        const bool negl = (mag == 0.0) || (fabs(app) + 100.0 * mag == fabs(app) && fabs(aqq) + 100.0 * mag == fabs(aqq));
+        if (!negl) {
+          const double theta = (aqq - app) / (2.0 * mag);
+          double t = 1.0 / (fabs(theta) + sqrt(theta * theta + 1.0));
+          if (theta < 0.0) t = -t;
+          g.cs = 1.0 / sqrt(t * t + 1.0);
+          g.sn = t * g.cs;
+          g.om = make_double2(apq.x / mag, -apq.y / mag);
+          any_rot = 1;
+        }
+        rr[q] = g;
+      }
+      __syncthreads();
+      // 2x2 blocks (pair P1 rows, pair P2 cols), P1 >= P2: A' = G1^H B G2
+      const int nblk = half * (half + 1) / 2;
+      for (int e = threadIdx.x; e < nblk; e += blockDim.x) {
+        int q1 = (int)((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
+        while (q1 * (q1 + 1) / 2 > e) --q1;
+        while ((q1 + 1) * (q1 + 2) / 2 <= e) ++q1;
+        const int q2 = e - q1 * (q1 + 1) / 2;
+        const JacRot g1 = rr[q1], g2 = rr[q2];
+        int k0, k1, l0, l1;
+        rr_pair(m, r, q1, k0, k1);
+        rr_pair(m, r, q2, l0, l1);
+        if (q1 == q2) {
+          const double app = a[pk(k0, k0)].x, aqq = a[pk(k1, k1)].x;
+          const double2 apq = ld_h(a, k0, k1);
+          const double mag = hypot(apq.x, apq.y);
+          if (g1.sn != 0.0) {
+            const double t = g1.sn / g1.cs;
+            a[pk(k0, k0)] = make_double2(app - t * mag, 0.0);
+            a[pk(k1, k1)] = make_double2(aqq + t * mag, 0.0);
+            st_h(a, k1, k0, make_double2(0.0, 0.0));
+          }
+          continue;
+        }
+        // G = [[cs, sn], [-sn om, cs om]] (rows: old index, cols: new index)
+        double2 B00 = ld_h(a, k0, l0), B01 = ld_h(a, k0, l1), B10 = ld_h(a, k1, l0), B11 = ld_h(a, k1, l1);
+        // right multiply by G2: columns l0, l1
+        const double2 om2 = g2.om;
+        auto cm = [](double2 x, double2 y) { return make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x); };
+        double2 t10 = cm(B01, om2), t11 = cm(B11, om2);
+        double2 C00 = make_double2(g2.cs * B00.x - g2.sn * t10.x, g2.cs * B00.y - g2.sn * t10.y);
+        double2 C01 = make_double2(g2.sn * B00.x + g2.cs * t10.x, g2.sn * B00.y + g2.cs * t10.y);
+        double2 C10 = make_double2(g2.cs * B10.x - g2.sn * t11.x, g2.cs * B10.y - g2.sn * t11.y);
+        double2 C11 = make_double2(g2.sn * B10.x + g2.cs * t11.x, g2.sn * B10.y + g2.cs * t11.y);
+        // left multiply by G1^H: rows k0, k1; G1^H = [[cs, -sn conj(om)], [sn, cs conj(om)]]
+        const double2 oc = make_double2(g1.om.x, -g1.om.y);
+        double2 u0 = cm(C10, oc), u1 = cm(C11, oc);
+        double2 D00 = make_double2(g1.cs * C00.x - g1.sn * u0.x, g1.cs * C00.y - g1.sn * u0.y);
+        double2 D01 = make_double2(g1.cs * C01.x - g1.sn * u1.x, g1.cs * C01.y - g1.sn * u1.y);
+        double2 D10 = make_double2(g1.sn * C00.x + g1.cs * u0.x, g1.sn * C00.y + g1.cs * u0.y);
+        double2 D11 = make_double2(g1.sn * C01.x + g1.cs * u1.x, g1.sn * C01.y + g1.cs * u1.y);
+        st_h(a, k0, l0, D00);
+        st_h(a, k0, l1, D01);
+        st_h(a, k1, l0, D10);
+        st_h(a, k1, l1, D11);
+      }
+      // record the round for the eigenvector replay
+      for (int q = threadIdx.x; q < half; q += blockDim.x) rotb[(size_t)rounds * half + q] = rr[q];
+      __syncthreads();
+      ++rounds;
+    }
+    __syncthreads();
+    const int cont = any_rot;
+    __syncthreads();
+    if (!cont) break;
+  }
+  if (threadIdx.x == 0) {
+    nrounds_out[b] = rounds;
+    if (sweep >= kJacMaxSweeps) latch_error(status, HFB_ERR_NO_CONVERGENCE);
+  }
+  for (int k = threadIdx.x; k < n; k += blockDim.x) w[(size_t)b * n + k] = a[pk(k, k)].x;
+}
+
+// Replay: V = I * G_1 * G_2 * ...; one CTA per (matrix, block of 8 rows);
+// then permute columns into ascending eigenvalue order.
+__global__ void __launch_bounds__(256)
+jacobi_vectors_kernel(int n, int lda, const JacRot* __restrict__ rot, const int* __restrict__ nrounds,
+                      const double* __restrict__ w, double2* V, size_t rot_stride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int RB = 8;
+  const int nb = (n + RB - 1) / RB;
+  const int b = blockIdx.x / nb, rb = blockIdx.x % nb;
+  const int m = n + (n & 1), half = m / 2;
+  double2* v = reinterpret_cast<double2*>(smem_raw);   // [RB][m]
+  int* order = reinterpret_cast<int*>(v + (size_t)RB * m);
+  const int r0 = rb * RB;
+  for (int e = threadIdx.x; e < RB * m; e += blockDim.x) {
+    const int i = e / m, j = e % m;
+    v[e] = make_double2((r0 + i) == j ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  const JacRot* rb_ = rot + (size_t)b * rot_stride;
+  const int nr = nrounds[b];
+  for (int r = 0; r < nr; ++r) {
+    const int rr_ = r % (m - 1);
+    for (int e = threadIdx.x; e < RB * half; e += blockDim.x) {
+      const int i = e / half, q = e % half;
+      const JacRot g = rb_[(size_t)r * half + q];
+      if (g.sn == 0.0) continue;
+      int p_, q_;
+      rr_pair(m, rr_, q, p_, q_);
+      const double2 vp = v[i * m + p_], vq = v[i * m + q_];
+      const double2 t = make_double2(vq.x * g.om.x - vq.y * g.om.y, vq.x * g.om.y + vq.y * g.om.x);
+      v[i * m + p_] = make_double2(g.cs * vp.x - g.sn * t.x, g.cs * vp.y - g.sn * t.y);
+      v[i * m + q_] = make_double2(g.sn * vp.x + g.cs * t.x, g.sn * vp.y + g.cs * t.y);
+    }
+    __syncthreads();
+  }
+  // ascending order of eigenvalues (stable: ties keep index order)
+  const double* wb = w + (size_t)b * n;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    int rank = 0;
+    const double wj = wb[j];
+    for (int k = 0; k < n; ++k) {
+      const double wk = wb[k];
+      rank += (wk < wj) || (wk == wj && k < j);
+    }
+    order[rank] = j;
+  }
+  __syncthreads();
+  double2* Vb = V + (size_t)b * n * lda;
+  for (int e = threadIdx.x; e < RB * n; e += blockDim.x) {
+    const int i = e / n, c = e % n;
+    if (r0 + i < n) Vb[(size_t)(r0 + i) * lda + c] = v[i * m + order[c]];
+  }
+}
+
+__global__ void sort_values_kernel(int n, int nb, double* w) {
+  const int b = blockIdx.x;
+  extern __shared__ double tmpw[];
+  double* wb = w + (size_t)b * n;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) tmpw[j] = wb[j];
+  __syncthreads();
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    int rank = 0;
+    const double wj = tmpw[j];
+    for (int k = 0; k < n; ++k) rank += (tmpw[k] < wj) || (tmpw[k] == wj && k < j);
+    wb[rank] = wj;
+  }
+}
+
+// nb matrices a[nb][n][lda] -> w[nb][n] ascending, v[nb][n][lda].
+int eigh_launch(hfb_ctx_s* c, int nb, int n, int lda, const double2* a, double* w, double2* v, cudaStream_t st) {
+  if (nb <= 0 || n <= 0) return HFB_OK;
+  const int m = n + (n & 1);
+  const size_t smem = sizeof(double2) * (size_t)m * (m + 1) / 2 + sizeof(JacRot) * (m / 2);
+  if (smem > 227 * 1024) return HFB_ERR_ARG;
+  const size_t rot_stride = (size_t)kJacMaxSweeps * (m - 1) * (m / 2);
+  char* buf = (char*)scratch(c, hfb_ctx_s::S_MAT, sizeof(JacRot) * rot_stride * nb + sizeof(int) * nb + 64);
+  if (!buf) return HFB_ERR_ALLOC;
+  JacRot* rot = (JacRot*)buf;
+  int* nr = (int*)(buf + sizeof(JacRot) * rot_stride * nb);
+  cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  jacobi_kernel<<<nb, 1024, smem, st>>>(n, lda, a, w, rot, nr, c->dev_status, rot_stride);
+  HFB_CHECK_LAUNCH();
+  const size_t smem2 = sizeof(double2) * 8 * m + sizeof(int) * m;
+  jacobi_vectors_kernel<<<nb * ((n + 7) / 8), 256, smem2, st>>>(n, lda, rot, nr, w, v, rot_stride);
+  HFB_CHECK_LAUNCH();
+  sort_values_kernel<<<nb, 256, sizeof(double) * n, st>>>(n, nb, w);
+  HFB_CHECK_LAUNCH();
+  return HFB_OK;
+}
+
+// ========================================================= small GEMMs ====
+// C[b] = A'[b] B'[b] with A' = A or A^H, B' = B or B^H; n x n, leading dim ld.
+// Batched over blockIdx.z with per-batch strides (elements).
+__global__ void zgemm_small_kernel(int n, int ld, int ta, int tb, const double2* A, size_t sa, const double2* B,
+                                   size_t sb, double2* C, size_t sc, Pair2 nper) {
+  __shared__ double2 As[16][17], Bs[16][17];
+  const int b = blockIdx.z;
+  const int nb = nper.v[b] > 0 ? nper.v[b] : n;
+  const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
+  if (blockIdx.y * 16 >= nb || blockIdx.x * 16 >= nb) return;
+  const double2* Ab = A + b * sa;
+  const double2* Bb = B + b * sb;
+  double re = 0, im = 0;
+  for (int k0 = 0; k0 < nb; k0 += 16) {
+    const int ka = k0 + threadIdx.x, kb = k0 + threadIdx.y;
+    double2 av = make_double2(0, 0), bv = make_double2(0, 0);
+    if (i < nb && ka < nb) {
+      if (ta) { av = Ab[(size_t)ka * ld + i]; av.y = -av.y; }
+      else av = Ab[(size_t)i * ld + ka];
+    }
+    if (j < nb && kb < nb) {
+      if (tb) { bv = Bb[(size_t)j * ld + kb]; bv.y = -bv.y; }
+      else bv = Bb[(size_t)kb * ld + j];
+    }
+    As[threadIdx.y][threadIdx.x] = av;
+    Bs[threadIdx.y][threadIdx.x] = bv;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const double2 x = As[threadIdx.y][k], y = Bs[k][threadIdx.x];
+      re += x.x * y.x - x.y * y.y;
+      im += x.x * y.y + x.y * y.x;
+    }
+    __syncthreads();
+  }
+  if (i < nb && j < nb) C[b * sc + (size_t)i * ld + j] = make_double2(re, im);
+}
+
+static int zgemm_small(int nmax, int ld, int ta, int tb, const double2* A, size_t sa, const double2* B, size_t sb,
+                       double2* C, size_t sc, Pair2 nper, int batch, cudaStream_t st) {
+  dim3 grid((nmax + 15) / 16, (nmax + 15) / 16, batch);
+  zgemm_small_kernel<<<grid, dim3(16, 16), 0, st>>>(nmax, ld, ta, tb, A, sa, B, sb, C, sc, nper);
+  HFB_CHECK_LAUNCH();
+  return HFB_OK;
+}
+
+// T = V diag(1/sqrt(max(w, thr))) with thr = max(1e-12, eps max(w) n) (static.py:473-479)
+__global__ void loewdin_scale_kernel(int ld, Pair2 nper, const double* w, size_t sw, const double2* V,
+                                     double2* T, size_t sm) {
+  const int b = blockIdx.y;
+  const int n = nper.v[b];
+  const double* wb = w + b * sw;
+  __shared__ double thr;
+  if (threadIdx.x == 0) {
+    double mx = wb[0];
+    for (int k = 1; k < n; ++k) mx = fmax(mx, wb[k]);
+    thr = fmax(1e-12, 2.220446049250313e-16 * mx * n);
+  }
+  __syncthreads();
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += gridDim.x * blockDim.x) {
+    const int i = e / n, j = e % n;
+    const double s = 1.0 / sqrt(fmax(wb[j], thr));
+    const double2 v = V[b * sm + (size_t)i * ld + j];
+    T[b * sm + (size_t)i * ld + j] = make_double2(v.x * s, v.y * s);
+  }
+}
+
+// Copy the diagonal's real part (sp_norm), and the lower-Hermitian lambda.
+__global__ void diag_real_kernel(int ld, Pair2 nper, Pair2 off, const double2* S, size_t sm, double* out) {
+  const int b = blockIdx.x;
+  for (int k = threadIdx.x; k < nper.v[b]; k += blockDim.x) out[off.v[b] + k] = S[b * sm + (size_t)k * ld + k].x;
+}
+
+// construct_hfb_matrices after h, gap are in the new basis (static.py:511-575).
+// One CTA per isospin.  H, G: [b][ld][ld]; writes hmatrix, gapmatrix,
+// symcond, lambda_save [b][nmax][nmax], sp_energy, deltaf, efluct.
+__global__ void __launch_bounds__(1024)
+lambda_kernel(int ld, int nmax, Pair2 nper, Pair2 off, int ipair, int tbcs, const double2* H,
+              const double2* G, size_t sm, const double* wocc, const double* wguv, const double* pairwg,
+              const double* wstates, double2* hmat, double2* gmat, double2* symc, double2* lsave, double* sp_energy,
+              double* deltaf, double* efluct) {
+  const int b = blockIdx.x;
+  const int n = nper.v[b], o = off.v[b];
+  __shared__ double red_max[32], red_sum[32];
+  const double2* Hb = H + b * sm;
+  const double2* Gb = G + b * sm;
+  double mx = 0.0, sm2 = 0.0;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e / n, j = e % n;
+    const double2 h = Hb[(size_t)i * ld + j];
+    const double2 ht = Hb[(size_t)j * ld + i];
+    double2 g = ipair ? Gb[(size_t)i * ld + j] : make_double2(0, 0);
+    double2 gt = ipair ? Gb[(size_t)j * ld + i] : make_double2(0, 0);
+    hmat[((size_t)b * nmax + i) * nmax + j] = h;
+    if (tbcs && i != j) { g = make_double2(0, 0); }
+    if (tbcs && i != j) { gt = make_double2(0, 0); }
+    gmat[((size_t)b * nmax + i) * nmax + j] = g;
+    // lambda_ij = w_j h_ij - wuv_j g_ij ; lambda^H_ij = conj(lambda_ji)
+    const double wj = wocc[o + j] * wstates[o + j], wi = wocc[o + i] * wstates[o + i];
+    const double uj = wguv[o + j] * pairwg[o + j] * wstates[o + j];
+    const double ui = wguv[o + i] * pairwg[o + i] * wstates[o + i];
+    const double2 l = make_double2(wj * h.x - uj * g.x, wj * h.y - uj * g.y);
+    const double2 lt = make_double2(wi * ht.x - ui * gt.x, -(wi * ht.y - ui * gt.y));   // conj(lambda_ji)
+    const double2 as = make_double2(0.5 * (l.x - lt.x), 0.5 * (l.y - lt.y));
+    const double2 sy = make_double2(0.5 * (l.x + lt.x), 0.5 * (l.y + lt.y));
+    symc[((size_t)b * nmax + i) * nmax + j] = as;
+    lsave[((size_t)b * nmax + i) * nmax + j] = sy;
+    const double ab = hypot(as.x, as.y);
+    mx = fmax(mx, ab);
+    sm2 += ab * ab;
+  }
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    sp_energy[o + k] = Hb[(size_t)k * ld + k].x;
+    if (ipair) deltaf[o + k] = Gb[(size_t)k * ld + k].x * pairwg[o + k];
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, s));
+    sm2 += __shfl_xor_sync(0xffffffffu, sm2, s);
+  }
+  if (threadIdx.x % 32 == 0) { red_max[threadIdx.x / 32] = mx; red_sum[threadIdx.x / 32] = sm2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, s = 0;
+    for (int k = 0; k < (int)(blockDim.x / 32); ++k) { a = fmax(a, red_max[k]); s += red_sum[k]; }
+    efluct[b] = a;
+    efluct[2 + b] = sqrt(s / ((double)n * n));
+  }
+}
+
+// lsave [b][nmax][nmax] -> L [b][ld][ld] (lambda used for the Lagrange update)
+__global__ void copy_lambda_kernel(int ld, int nmax, Pair2 nper, const double2* lsave, double2* L, size_t sm) {
+  const int b = blockIdx.y;
+  const int n = nper.v[b];
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += gridDim.x * blockDim.x) {
+    const int i = e / n, j = e % n;
+    L[b * sm + (size_t)i * ld + j] = lsave[((size_t)b * nmax + i) * nmax + j];
+  }
+}
+
+// ============================================================== rotate ====
+// out1_j = sum_i psi_i U_ij, out2_j = sum_i psi_i L_ij for states of one
+// isospin block; tile 64 (k) x 32 (j) per CTA, 256 threads (8 outputs each).
+template <class R>
+__global__ void __launch_bounds__(256)
+rotate_kernel(int ns, size_t K, const cplx<R>* __restrict__ psi, const double2* __restrict__ U,
+              const double2* __restrict__ L, int ld, cplx<R>* out1, cplx<R>* out2) {
+  using Z = cplx<R>;
+  constexpr int KT = 64, JT = 32, IT = 16;
+  __shared__ Z Ps[IT][KT + 1];
+  __shared__ Z Ws[IT][JT + 1];
+  const int njt = (2 * ns + JT - 1) / JT;
+  const int jt = blockIdx.x % njt;
+  const size_t k0 = (size_t)(blockIdx.x / njt) * KT;
+  const int j0 = jt * JT;
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;   // tx -> k rows (2), ty -> j columns (4)
+  R acc[2][4][2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[u][v][0] = acc[u][v][1] = R(0);
+  for (int i0 = 0; i0 < ns; i0 += IT) {
+    for (int e = threadIdx.x; e < IT * KT; e += 256) {
+      const int ii = e / KT, kk = e % KT;
+      const size_t k = k0 + kk;
+      Ps[ii][kk] = (i0 + ii < ns && k < K) ? psi[(size_t)(i0 + ii) * K + k] : czero<Z>();
+    }
+    for (int e = threadIdx.x; e < IT * JT; e += 256) {
+      const int ii = e / JT, jj = e % JT;
+      const int j = j0 + jj;
+      double2 v = make_double2(0, 0);
+      if (i0 + ii < ns && j < 2 * ns) v = j < ns ? U[(size_t)(i0 + ii) * ld + j] : L[(size_t)(i0 + ii) * ld + (j - ns)];
+      Ws[ii][jj] = mk<R>((R)v.x, (R)v.y);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ii = 0; ii < IT; ++ii) {
+      Z pv[2], wv[4];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) pv[u] = Ps[ii][tx + 32 * u];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) wv[v] = Ws[ii][ty + 8 * v];
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          acc[u][v][0] += pv[u].x * wv[v].x - pv[u].y * wv[v].y;
+          acc[u][v][1] += pv[u].x * wv[v].y + pv[u].y * wv[v].x;
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const int j = j0 + ty + 8 * v;
+    if (j >= 2 * ns) continue;
+    Z* o = j < ns ? out1 + (size_t)j * K : out2 + (size_t)(j - ns) * K;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const size_t k = k0 + tx + 32 * u;
+      if (k < K) o[k] = mk<R>(acc[u][v][0], acc[u][v][1]);
+    }
+  }
+}
+
+int rotate_launch(hfb_ctx_s* c, int prec, int s0, int ns, const void* psi, const double2* U, const double2* L, int ld,
+                  void* out1, void* out2, cudaStream_t st) {
+  if (ns <= 0) return HFB_OK;
+  const size_t K = (size_t)2 * c->n * c->n * c->n;
+  const int njt = (2 * ns + 31) / 32;
+  const size_t nkt = (K + 63) / 64;
+  const size_t off = (size_t)s0 * K;
+  if (prec == HFB_F64)
+    rotate_kernel<double><<<(unsigned)(nkt * njt), 256, 0, st>>>(ns, K, (const double2*)psi + off, U, L, ld,
+                                                                 (double2*)out1 + off, (double2*)out2 + off);
+  else
+    rotate_kernel<float><<<(unsigned)(nkt * njt), 256, 0, st>>>(ns, K, (const float2*)psi + off, U, L, ld,
+                                                                (float2*)out1 + off, (float2*)out2 + off);
+  HFB_CHECK_LAUNCH();
+  return HFB_OK;
+}
+
+}  // namespace hfb
+
+using namespace hfb;
+
+extern "C" int hfb_gram(hfb_ctx_t ctx, int prec, int s0, int ns, int mask, const void* psi, const void* hampsi,
+                        const void* hmfpsi, const double* v_pair_iq, double wxyz, double* out, void* stream) {
+  if (!ctx || !psi || !out || ns <= 0) return HFB_ERR_ARG;
+  if (((mask & 2) && !hampsi) || ((mask & 4) && !hmfpsi) || ((mask & 8) && !v_pair_iq)) return HFB_ERR_ARG;
+  return gram_launch(ctx, prec, s0, ns, mask, psi, hampsi, hmfpsi, v_pair_iq, wxyz, (double2*)out, ns,
+                     as_stream(stream));
+}
+
+extern "C" int hfb_eigh(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w, double* v, void* stream) {
+  if (!ctx || !a || !w || !v || n <= 0 || lda < n) return HFB_ERR_ARG;
+  return eigh_launch(ctx, nb, n, lda, (const double2*)a, w, (double2*)v, as_stream(stream));
+}
+
+extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, void* stream) {
+  if (!ctx || !a || !a->psi || !a->psi_out || a->psi_out == a->psi || !a->lagrange || !a->sp_norm || !a->lambda_save) return HFB_ERR_ARG;
+  if (a->diagonalize && !a->hampsi) return HFB_ERR_ARG;
+  if (a->construct && (!a->hmfpsi || !a->sp_energy || !a->hmatrix || !a->gapmatrix || !a->symcond || !a->efluct))
+    return HFB_ERR_ARG;
+  if (a->construct && a->ipair && (!a->v_pair || !a->deltaf)) return HFB_ERR_ARG;
+  cudaStream_t st = as_stream(stream);
+  const int n0 = a->npsi[0], n1 = a->npsi[1];
+  const int ld = n0 > n1 ? n0 : n1;
+  const size_t sm = (size_t)ld * ld;
+  const size_t n3 = (size_t)ctx->n * ctx->n * ctx->n;
+  // workspace: 4 Gram matrices + 8 work matrices per isospin, eigenvalues, small ints
+  const size_t nmat = 2 * (4 + 8);
+  char* ws = (char*)scratch(ctx, hfb_ctx_s::S_SMALL, sizeof(double2) * nmat * sm + sizeof(double) * 4 * ld);
+  if (!ws) return HFB_ERR_ALLOC;
+  double2* gm = (double2*)ws;                 // [iq][4][ld][ld]: S, Lambda, H_old, G_old
+  double2* V = gm + 2 * 4 * sm;               // [iq][ld][ld] eigenvectors of S
+  double2* T = V + 2 * sm;                    // scratch
+  double2* Ur = T + 2 * sm;                   // S^-1/2
+  double2* Vl = Ur + 2 * sm;                  // eigenvectors of lambda
+  double2* U = Vl + 2 * sm;                   // total transform
+  double2* Hn = U + 2 * sm;                   // U^H H U
+  double2* Gn = Hn + 2 * sm;                  // U^H G U
+  double2* Lw = Gn + 2 * sm;                  // U lambda
+  double* w = (double*)(Lw + 2 * sm);         // [iq][ld] (x2: S and lambda)
+  Pair2 nper, off;
+  nper.v[0] = n0; nper.v[1] = n1;
+  off.v[0] = 0; off.v[1] = n0;
+  const int nq[2] = {n0, n1}, so[2] = {0, n0};
+  int r;
+  for (int iq = 0; iq < 2; ++iq) {
+    int mask = 1;
+    if (a->diagonalize) mask |= 2;
+    if (a->construct) mask |= 4;
+    if (a->construct && a->ipair) mask |= 8;
+    r = gram_launch(ctx, prec, so[iq], nq[iq], mask, a->psi, a->hampsi, a->hmfpsi,
+                    a->v_pair ? a->v_pair + (size_t)iq * n3 : nullptr, a->wxyz, gm + (size_t)iq * 4 * sm, ld, st);
+    if (r) return r;
+  }
+  diag_real_kernel<<<2, 256, 0, st>>>(ld, nper, off, gm, 4 * sm, a->sp_norm);
+  HFB_CHECK_LAUNCH();
+  // eigh(S) for both isospins (lower triangle)
+  for (int iq = 0; iq < 2; ++iq) {
+    r = eigh_launch(ctx, 1, nq[iq], ld, gm + (size_t)iq * 4 * sm, w + (size_t)iq * ld, V + (size_t)iq * sm, st);
+    if (r) return r;
+  }
+  loewdin_scale_kernel<<<dim3(64, 2), 256, 0, st>>>(ld, nper, w, ld, V, T, sm);
+  HFB_CHECK_LAUNCH();
+  r = zgemm_small(ld, ld, 0, 1, T, sm, V, sm, Ur, sm, nper, 2, st);
+  if (r) return r;
+  double2* Uuse = Ur;
+  if (a->diagonalize) {
+    for (int iq = 0; iq < 2; ++iq) {
+      r = eigh_launch(ctx, 1, nq[iq], ld, gm + (size_t)iq * 4 * sm + sm, w + 2 * ld + (size_t)iq * ld,
+                      Vl + (size_t)iq * sm, st);
+      if (r) return r;
+    }
+    r = zgemm_small(ld, ld, 0, 0, Ur, sm, Vl, sm, U, sm, nper, 2, st);
+    if (r) return r;
+    Uuse = U;
+  }
+  const int nmax = a->nmax;
+  if (a->construct) {
+    // H = U^H (H_old U), G likewise
+    r = zgemm_small(ld, ld, 0, 0, gm + 2 * sm, 4 * sm, Uuse, sm, T, sm, nper, 2, st);
+    if (r) return r;
+    r = zgemm_small(ld, ld, 1, 0, Uuse, sm, T, sm, Hn, sm, nper, 2, st);
+    if (r) return r;
+    if (a->ipair) {
+      r = zgemm_small(ld, ld, 0, 0, gm + 3 * sm, 4 * sm, Uuse, sm, T, sm, nper, 2, st);
+      if (r) return r;
+      r = zgemm_small(ld, ld, 1, 0, Uuse, sm, T, sm, Gn, sm, nper, 2, st);
+      if (r) return r;
+    }
+    lambda_kernel<<<2, 1024, 0, st>>>(ld, nmax, nper, off, a->ipair, a->tbcs, Hn, Gn, sm, a->wocc, a->wguv, a->pairwg,
+                                      a->wstates, (double2*)a->hmatrix, (double2*)a->gapmatrix, (double2*)a->symcond,
+                                      (double2*)a->lambda_save, a->sp_energy, a->deltaf, a->efluct);
+    HFB_CHECK_LAUNCH();
+  }
+  // L = U lambda_save (lambda_save just written when construct)
+  copy_lambda_kernel<<<dim3(64, 2), 256, 0, st>>>(ld, nmax, nper, (const double2*)a->lambda_save, T, sm);
+  HFB_CHECK_LAUNCH();
+  r = zgemm_small(ld, ld, 0, 0, Uuse, sm, T, sm, Lw, sm, nper, 2, st);
+  if (r) return r;
+  for (int iq = 0; iq < 2; ++iq) {
+    r = rotate_launch(ctx, prec, so[iq], nq[iq], a->psi, Uuse + (size_t)iq * sm, Lw + (size_t)iq * sm, ld, a->psi_out,
+                      a->lagrange, st);
+    if (r) return r;
+  }
+  return HFB_OK;
+}

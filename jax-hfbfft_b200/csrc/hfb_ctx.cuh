@@ -1,0 +1,55 @@
+// Library context: grid, device constants and the scratch arena.
+#pragma once
+#include <cuda_runtime.h>
+#include "../../include/hfb.h"
+#include "hfb_common.cuh"
+
+struct hfb_ctx_s {
+  int n;                 // cubic grid size
+  double d[3];           // spacings dx, dy, dz
+  double wxyz;
+  int periodic;
+  int nstmax;
+  int n2;                // Coulomb grid size (2n, or n when periodic)
+  double* der1[3];       // dense spectral derivative matrices (grids.py:36-61)
+  double* der2[3];
+  double2* coul_q;       // Green's function in k space, n2^3 (coulomb.py:23-52)
+  int* dev_status;       // latched device-side error code
+  // scratch arena: fixed slots, grown on demand (never shrunk)
+  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_NSLOT };
+  void* slot[S_NSLOT];
+  size_t slot_bytes[S_NSLOT];
+};
+
+namespace hfb {
+
+// Scratch buffer ``s`` of at least ``bytes``; nullptr on allocation failure.
+void* scratch(hfb_ctx_s* c, int s, size_t bytes);
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+#define HFB_CHECK_LAUNCH()                                            \
+  do {                                                                \
+    cudaError_t e_ = cudaGetLastError();                              \
+    if (e_ != cudaSuccess) return HFB_ERR_CUDA;                       \
+  } while (0)
+
+// Supported cubic grid sizes; ``fn`` is a generic lambda taking
+// std::integral_constant<int, N>.
+template <class F>
+int dispatch_n(int n, F&& fn) {
+  switch (n) {
+    case 8: return fn(std::integral_constant<int, 8>{});
+    case 16: return fn(std::integral_constant<int, 16>{});
+    case 24: return fn(std::integral_constant<int, 24>{});
+    case 32: return fn(std::integral_constant<int, 32>{});
+    case 40: return fn(std::integral_constant<int, 40>{});
+    case 48: return fn(std::integral_constant<int, 48>{});
+    default: return HFB_ERR_UNSUPPORTED_GRID;
+  }
+}
+
+// Device-side error latch (first error wins).
+__device__ __forceinline__ void latch_error(int* st, int code) { atomicCAS(st, 0, code); }
+
+}  // namespace hfb

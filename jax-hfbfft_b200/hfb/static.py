@@ -1,0 +1,284 @@
+"""Static iteration: initial states, gradient step, diagonalisation step and
+the driver loop (mirror of static.py of jax-hfbfft).
+
+All array work runs in libhfb on the device; the host keeps the reference's
+control flow (static.py:1666-1882) and reads a handful of scalars once per
+iteration (E_bind, the fluctuation measures) for the convergence test and
+the step-size adaptation.
+"""
+from dataclasses import dataclass, field
+import math
+import time
+
+import torch
+
+from . import _lib
+from ._lib import call, ptr, stream_ptr, prec_of, GrstepArgs, DiagArgs
+from .densities import add_density
+from .meanfield import skyrme
+from .pairs import pair
+from .energies import integ_energy, sum_energy
+from .inout import sp_properties
+
+
+@dataclass
+class Static:
+    tdiag: bool = False
+    tlarge: bool = False
+    tvaryx_0: bool = False
+    ttime: bool = False
+    tsort: bool = False
+    maxiter: int = 40
+    iternat: int = 0
+    iternat_start: int = 40
+    iteranneal: int = 0
+    pairenhance: float = 0.0
+    inibcs: int = 30
+    inidiag: int = 30
+    delstepbas: float = 2.0
+    e0bas: float = 10.0
+    outerpot: int = 0
+    radinx: float = 3.1
+    radiny: float = 3.1
+    radinz: float = 3.1
+    serr: float = 1.0e-20
+    x0dmp: float = 0.45
+    e0dmp: float = 100.0
+    x0dmpmin: float = 0.45
+    outertype: str = "N"
+    hmatrix: torch.Tensor = None
+    gapmatrix: torch.Tensor = None
+    symcond: torch.Tensor = None
+    lambda_save: torch.Tensor = None
+    sums_dev: torch.Tensor = None      # running sumflu, delesum on the device
+
+    @property
+    def sumflu(self):
+        return float(self.sums_dev[0])
+
+    @property
+    def delesum(self):
+        return float(self.sums_dev[1])
+
+
+def init_static(forces, levels, **kwargs):
+    """static.py:53-90 (also rescales h2m by (A-1)/A when zpe == 0)."""
+    known = set(Static.__dataclass_fields__)
+    st = Static(**{k: v for k, v in kwargs.items() if k in known})
+    st.x0dmpmin = st.x0dmp
+    nst = max(levels.npsi)
+    for k in ("hmatrix", "gapmatrix", "symcond", "lambda_save"):
+        setattr(st, k, torch.zeros((2, nst, nst), dtype=torch.complex128, device="cuda"))
+    st.sums_dev = torch.zeros(4, dtype=torch.float64, device="cuda")
+    if forces.zpe == 0:
+        a = levels.mass_number
+        forces.h2m = [h * (a - 1.0) / a for h in forces.h2m]
+    return forces, st
+
+
+def ho_quantum_numbers(nps):
+    """(i, j, k) of the first ``nps`` states of one isospin, two spins per
+    triple, shells ka = i + j + k ordered with loops k, j, i (static.py:619-660)."""
+    out = []
+    for ka in range(nps + 10):
+        for k in range(ka + 1):
+            for j in range(ka + 1):
+                for i in range(ka + 1):
+                    if ka == i + j + k:
+                        for _ in range(2):
+                            if len(out) >= nps:
+                                return out
+                            out.append((i, j, k))
+    return out
+
+
+def harmosc(grids, levels, params, static):
+    """Gaussian x monomial initial states (static.py:580-738), built on the
+    device; occupations reset to the first N / Z states of each isospin."""
+    qn = []
+    for iq in range(2):
+        tr = ho_quantum_numbers(levels.npsi[iq])
+        for off in range(levels.npsi[iq]):
+            i, j, k = tr[off]
+            qn.append((i, j, k, off % 2))
+    qd = torch.tensor(qn, dtype=torch.int32, device="cuda").contiguous()
+    call("hfb_harmosc", grids.ctx.handle, prec_of(levels.psi), levels.nstmax, ptr(qd), float(static.radinx),
+         float(static.radiny), float(static.radinz), ptr(levels.psi), stream_ptr())
+    levels.wocc.zero_()
+    levels.wocc[:levels.nneut] = 1.0
+    levels.wocc[levels.npsi[0]:levels.npsi[0] + levels.nprot] = 1.0
+    levels.wguv.zero_()
+    return levels
+
+
+def grstep(forces, grids, levels, meanfield, params, static):
+    """Damped-gradient step for every state (static.py:93-259)."""
+    lv = levels
+    rd = torch.float64 if lv.psi.dtype == torch.complex128 else torch.float32
+    if meanfield.pot.dtype != rd:
+        meanfield.pack(lv.psi.dtype)
+    a = GrstepArgs()
+    a.nst, a.nneut = lv.nstmax, lv.npsi[0]
+    a.tbcs = int(bool(forces.tbcs))
+    a.use_lagrange = int(params.iteration > 1 and not forces.tbcs)
+    a.do_fluct = int(params.mprint > 0 and params.iteration % params.mprint == 0)
+    a.x0dmp, a.e0dmp, a.h2ma, a.wxyz = float(static.x0dmp), float(static.e0dmp), float(forces.h2ma), grids.wxyz
+    a.pot, a.v_pair = ptr(meanfield.pot), ptr(meanfield.v_pair)
+    a.psi, a.hampsi, a.hmfpsi, a.delpsi = ptr(lv.psi), ptr(lv.hampsi), ptr(lv.hmfpsi), ptr(lv.delpsi)
+    a.lagrange = ptr(lv.lagrange)
+    a.wocc, a.wguv, a.pairwg, a.wstates = ptr(lv.wocc), ptr(lv.wguv), ptr(lv.pairwg), ptr(lv.wstates)
+    a.sp_energy, a.sp_efluct1, a.sp_efluct2 = ptr(lv.sp_energy), ptr(lv.sp_efluct1), ptr(lv.sp_efluct2)
+    sums = static.sums_dev[2:4]
+    a.sums = ptr(sums)
+    call("hfb_grstep", grids.ctx.handle, prec_of(lv.psi), a, stream_ptr())
+    static.sums_dev[0:2] += sums
+    # delpsi = v_pair * psi_new (static.py:203, 250): diagstep forms it on the fly
+    lv._v_pair = meanfield.v_pair
+    return levels, static
+
+
+def diagstep(energies, forces, grids, levels, static, diagonalize=False, construct=True, npsi_neutron=None,
+             npsi_proton=None):
+    """Loewdin orthonormalisation, optional diagonalisation of lambda, h and
+    gap matrices in the new basis, lambda and the Lagrange fields
+    (static.py:261-577)."""
+    lv = levels
+    a = DiagArgs()
+    a.npsi[0], a.npsi[1] = lv.npsi
+    a.nmax = max(lv.npsi)
+    a.diagonalize, a.construct = int(bool(diagonalize)), int(bool(construct))
+    a.ipair, a.tbcs = int(forces.ipair), int(bool(forces.tbcs))
+    a.wxyz = grids.wxyz
+    a.psi, a.psi_out = ptr(lv.psi), ptr(lv.psi_spare)
+    a.hampsi, a.hmfpsi, a.lagrange = ptr(lv.hampsi), ptr(lv.hmfpsi), ptr(lv.lagrange)
+    vpair = getattr(lv, "_v_pair", None)
+    if vpair is None:   # before the first gradient step delpsi is zero (levels.py:69)
+        vpair = torch.zeros((2, grids.nx, grids.ny, grids.nz), dtype=torch.float64, device=lv.psi.device)
+    a.v_pair = ptr(vpair)
+    a.wocc, a.wguv, a.pairwg, a.wstates = ptr(lv.wocc), ptr(lv.wguv), ptr(lv.pairwg), ptr(lv.wstates)
+    a.sp_norm, a.sp_energy, a.deltaf = ptr(lv.sp_norm), ptr(lv.sp_energy), ptr(lv.deltaf)
+    a.hmatrix, a.gapmatrix = ptr(static.hmatrix), ptr(static.gapmatrix)
+    a.symcond, a.lambda_save = ptr(static.symcond), ptr(static.lambda_save)
+    a.efluct = ptr(energies.efluct_dev)
+    call("hfb_diagstep", grids.ctx.handle, prec_of(lv.psi), a, stream_ptr())
+    lv.psi, lv.psi_spare = lv.psi_spare, lv.psi
+    return energies, levels, static
+
+
+@dataclass
+class RunResult:
+    history: list = field(default_factory=list)
+    converged: bool = False
+    iterations: int = 0
+    seconds: float = 0.0
+
+
+def _energies(coulomb, densities, energies, forces, grids, levels, meanfield, params, pairs):
+    integ_energy(coulomb, densities, energies, forces, grids, levels, params, pairs)
+    sum_energy(energies, levels, meanfield, pairs, grids=grids)
+    return energies
+
+
+def prepare(coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs):
+    """Steps before the loop (static.py:1700-1744)."""
+    params.iteration = 0
+    diagstep(energies, forces, grids, levels, static, False, True)
+    add_density(densities, grids, levels)
+    skyrme(coulomb, densities, forces, grids, meanfield, params, static, dtype=levels.psi.dtype)
+    grstep(forces, grids, levels, meanfield, params, static)
+    if forces.ipair != 0:
+        pair(levels, meanfield, forces, params, grids, pairs)
+    diagstep(energies, forces, grids, levels, static, False, True)
+    sp_properties(forces, grids, levels, None)
+    _energies(coulomb, densities, energies, forces, grids, levels, meanfield, params, pairs)
+    if static.tvaryx_0:
+        static.x0dmp = static.x0dmp * 3.0
+    static._tbcssav = forces.tbcs
+    return energies
+
+
+def iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs,
+            x0_schedule=None):
+    """One pass of the loop body (static.py:1755-1882).  Returns True once
+    efluct1 < serr.  ``x0_schedule[k]`` (optional) forces the step size of
+    iteration k (the reference's adaptation compares max|lambda_asym|, which
+    depends on the eigenvector basis inside degenerate subspaces)."""
+    params.iteration = i
+    forces.tbcs = True if i <= static.inibcs else static._tbcssav
+    static.tdiag = not (i > static.inidiag)
+    grstep(forces, grids, levels, meanfield, params, static)
+    if forces.tbcs:
+        static.tdiag = True
+    diagstep(energies, forces, grids, levels, static, static.tdiag, True)
+    if forces.ipair != 0:
+        pair(levels, meanfield, forces, params, grids, pairs)
+    if forces.ipair != 0 and static.iternat > 0 and i > static.iternat_start and not forces.tbcs:
+        raise NotImplementedError("hfb_natural sub-iterations (static.py:920-1070) are not part of the hot path")
+    # densities with mixing 0.2 new + 0.8 old for rho, tau, chi, and the
+    # kinetic energies of sp_properties from the same derivatives
+    add_density(densities, grids, levels, mix=0.2, forces=forces)
+    skyrme(coulomb, densities, forces, grids, meanfield, params, static, dtype=levels.psi.dtype)
+    _energies(coulomb, densities, energies, forces, grids, levels, meanfield, params, pairs)
+    energies.sync()
+    grids.ctx.check(f"iteration {i}")
+    en = energies
+    if en.efluct1[0] < static.serr and i > 1:
+        return True
+    if static.tvaryx_0:
+        if ((en.ehf < en.ehfprev and en.efluct1[0] < en.efluct1prev * (1.0 - 1.0e-5))
+                or en.efluct2[0] < en.efluct2prev * (1.0 - 1.0e-5)):
+            static.x0dmp = static.x0dmp * 1.005
+        else:
+            static.x0dmp = static.x0dmp * 0.8
+        static.x0dmp = min(max(static.x0dmp, static.x0dmpmin), static.x0dmpmin * 5.0)
+        en.efluct1prev = en.efluct1[0]
+        en.efluct2prev = en.efluct2[0]
+        en.ehfprev = en.ehf
+    if x0_schedule is not None and i + 1 < len(x0_schedule):
+        static.x0dmp = float(x0_schedule[i + 1])
+    return False
+
+
+def statichf(coulomb, densities, energies, forces, grids, levels, meanfield, moment, params, static, pairs,
+             maxiter=None, x0_schedule=None, callback=None, de_tol=None):
+    """The self-consistent loop (static.py:1666-1882, without file output).
+
+    Stops on the reference's criterion efluct1 < serr, or, when ``de_tol`` is
+    given, once |E_bind(i) - E_bind(i-1)| < de_tol.  ``callback(i, energies)``
+    runs after every iteration.  Returns the reference's tuple plus a
+    RunResult with the per-iteration history."""
+    res = RunResult()
+    t0 = time.perf_counter()
+    prepare(coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs)
+    energies.sync()
+    res.history.append(dict(iteration=0, ehf=energies.ehf, ehfint=energies.ehfint, x0dmp=static.x0dmp))
+    n = static.maxiter if maxiter is None else maxiter
+    prev = energies.ehf
+    for i in range(1, n + 1):
+        x0_used = static.x0dmp
+        done = iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs,
+                       x0_schedule)
+        res.history.append(dict(iteration=i, ehf=energies.ehf, ehfint=energies.ehfint,
+                                efluct1=energies.efluct1[0], efluct2=energies.efluct2[0], x0dmp=x0_used,
+                                t=time.perf_counter() - t0))
+        res.iterations = i
+        if callback is not None:
+            callback(i, energies)
+        if de_tol is not None and abs(energies.ehf - prev) < de_tol and i > 1:
+            done = True
+        prev = energies.ehf
+        if done:
+            res.converged = True
+            break
+    torch.cuda.synchronize()
+    res.seconds = time.perf_counter() - t0
+    return (coulomb, densities, energies, forces, grids, levels, meanfield, moment, params, static, pairs), res
+
+
+def to_precision(state, dtype):
+    """Switch a running state dict (from hfb.config.setup) between the FP64
+    (complex128) and FP32 (complex64) paths: states are converted and the
+    hpsi potentials repacked; densities, matrices and energies stay FP64."""
+    state["levels"].to_precision(dtype)
+    state["meanfield"].pack(dtype)
+    return state

@@ -1,0 +1,117 @@
+"""C-ABI checks that need no GPU: every function declared in include/hfb.h is
+exported by libhfb.so and bound in hfb._lib; the ctypes structure layouts
+match the C compiler's; host-side set-up logic matches the oracle."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "hfb.h")
+
+
+def _declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(hfb_\w+)\s*\(", txt, re.M)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from hfb import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        import build as b
+        b.build()
+    return _lib.load()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    from hfb import _lib
+    names = _declared()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_lib.SYMBOLS)
+
+
+def test_status_strings(lib):
+    from hfb import _lib
+    for code in range(8):
+        assert lib.hfb_status_string(code).decode()
+    assert lib.hfb_status_string(4).decode().startswith("BCS")
+
+
+def test_ctx_create_rejects_bad_grids_without_gpu(lib):
+    h = C.c_void_p()
+    # non-cubic and odd grids are rejected before any device call
+    assert lib.hfb_ctx_create(16, 16, 24, 1.0, 1.0, 1.0, 0, 0, C.byref(h)) == 2
+    assert lib.hfb_ctx_create(15, 15, 15, 1.0, 1.0, 1.0, 0, 0, C.byref(h)) == 1
+    assert lib.hfb_ctx_create(20, 20, 20, 1.0, 1.0, 1.0, 0, 0, C.byref(h)) == 2
+
+
+def test_null_arguments_are_rejected(lib):
+    assert lib.hfb_hpsi(None, 0, None, 1, 1, None, None, None, None, None, None, None) == 1
+    assert lib.hfb_pair(None, None, None) == 1
+
+
+def test_struct_layouts_match_c():
+    """Compile a probe against include/hfb.h and compare sizeof / offsetof."""
+    from hfb import _lib
+    structs = {"hfb_force": _lib.HfbForce, "hfb_grstep_args": _lib.GrstepArgs, "hfb_diag_args": _lib.DiagArgs,
+               "hfb_pair_args": _lib.PairArgs}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0;}")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "probe.c")
+        exe = os.path.join(d, "probe")
+        open(src, "w").write("\n".join(lines))
+        subprocess.run(["gcc", src, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    got = {}
+    for ln in out.splitlines():
+        s, f, v = ln.split()
+        got[(s, f)] = int(v)
+    for cname, cls in structs.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
+
+
+def test_ho_quantum_numbers_match_oracle():
+    from hfb.static import ho_quantum_numbers
+    from oracle.static import ho_quantum_numbers as ref
+    for n in (1, 2, 10, 32, 96, 140):
+        assert ho_quantum_numbers(n) == ref(n)
+
+
+def test_force_coefficients_match_oracle():
+    from hfb.forces import init_forces
+    from oracle.model import init_forces as ref
+    for ipair in (0, 5, 6):
+        a = init_forces(None, name="SLy4", ipair=ipair)
+        b = ref("SLy4", ipair=ipair)
+        for k in ("b0", "b0p", "b1", "b1p", "b2", "b2p", "b3", "b3p", "b4", "b4p", "slate", "Crho0", "Crho1",
+                  "Crho0D", "Crho1D", "Cdrho0", "Cdrho1", "Ctau0", "Ctau1", "CdJ0", "CdJ1", "h2ma", "v0prot",
+                  "v0neut", "rho0pr"):
+            assert getattr(a, k) == pytest.approx(getattr(b, k), rel=1e-15, abs=1e-15), k
+        s = a.c_struct()
+        assert s.b0 == a.b0 and s.ipair == ipair
+
+
+def test_oscillator_radii():
+    from hfb.config import ho_radii, case_dict
+    rx, ry, rz = ho_radii(8, 8)
+    assert rx == ry == rz
+    assert abs(rx - 2.2576) < 1e-3      # radin = sqrt(2) b, b^2 = 2 h2m / (41 A^-1/3)
+    rx, ry, rz = ho_radii(24, 24, beta=0.2)
+    assert rz > rx and abs(rx * ry * rz - ho_radii(24, 24)[0] ** 3) < 1e-9
+    c = case_dict("Pb208")
+    assert c["levels"]["npsi"] == [140, 96] and c["grid"]["nx"] == 48

@@ -1,0 +1,296 @@
+"""CUDA kernels through the C ABI against the reference's golden vectors and
+the oracle.  Tolerances: FP64 paths 1e-11 relative (max |diff| / max |ref|);
+FP32 paths 3e-5 relative."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+from conftest import GOLDEN  # noqa: E402
+
+TOL64 = 1e-11
+TOL32 = 3e-5
+
+
+def rel(a, b):
+    a = a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+    b = b.detach().cpu().numpy() if isinstance(b, torch.Tensor) else np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def T(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    return t.to(dtype) if dtype is not None else t
+
+
+@pytest.fixture(scope="module")
+def unit():
+    return dict(np.load(os.path.join(GOLDEN, "unit_n8.npz")))
+
+
+@pytest.fixture(scope="module")
+def g8():
+    import hfb
+    from hfb import levels
+    p = hfb.params.init_params()
+    g = hfb.grids.init_grids(p, nx=8, ny=8, nz=8, dx=0.9, dy=0.9, dz=0.9)
+    levels.use_grid(g)
+    return g
+
+
+def _forces8():
+    import hfb
+    f = hfb.forces.init_forces(None, name="SLy4", ipair=6, tbcs=False, v0prot=362.0, v0neut=362.0, rho0pr=0.32)
+    a = 5   # the golden unit case has nneut = 3, nprot = 2 (h2m scaled by (A-1)/A)
+    f.h2m = [h * (a - 1.0) / a for h in f.h2m]
+    return f
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_cderv_against_reference(unit, g8, dtype):
+    from hfb import levels as L
+    tol = TOL64 if dtype == torch.complex128 else TOL32
+    psi = T(unit["in_psi"], dtype)
+    b = T(unit["in_b"])
+    for tag in ("x", "y", "z"):
+        assert rel(getattr(L, f"cderv{tag}00")(0.9, psi), unit[f"cderv{tag}00"]) < tol
+        d1, d2 = getattr(L, f"cderv{tag}01")(0.9, psi)
+        assert rel(d1, unit[f"cderv{tag}01_d1"]) < tol and rel(d2, unit[f"cderv{tag}01_d2"]) < tol
+        d1, d2 = getattr(L, f"cderv{tag}02")(0.9, psi, b)
+        assert rel(d1, unit[f"cderv{tag}02_d1"]) < tol and rel(d2, unit[f"cderv{tag}02_d2"]) < tol, tag
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_laplace_against_reference(unit, g8, dtype):
+    from hfb import levels as L
+    tol = TOL64 if dtype == torch.complex128 else TOL32
+    f = _forces8()
+    psi = T(unit["in_psi"], dtype)
+    assert rel(L.laplace(0, 0, g8, f, None, 1.0, 0.0, psi, 0.0, 100.0), unit["laplace_bcs"]) < tol
+    assert rel(L.laplace(0, 0, g8, f, None, 0.37, 0.02, psi, 3.5, 100.0), unit["laplace_hfb"]) < tol
+
+
+def _mf_from_unit(g, unit, dtype):
+    import hfb
+    mf = hfb.meanfield.init_meanfield(g, dtype)
+    for k in ("upot", "bmass", "v_pair", "aq", "spot", "wlspot"):
+        getattr(mf, k).copy_(T(unit[f"in_mf_{k}"]))
+    mf.pack(dtype)
+    return mf
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_hpsi01_against_reference(unit, g8, dtype):
+    import hfb
+    tol = TOL64 if dtype == torch.complex128 else 1e-4
+    mf = _mf_from_unit(g8, unit, dtype)
+    psi = T(unit["in_psi"], dtype)
+    for iq in range(2):
+        out = hfb.meanfield.hpsi01(g8, mf, iq, 0.8, 0.3, psi)
+        for o, tag in zip(out, ("pout", "mf", "del")):
+            assert rel(o, unit[f"hpsi_iq{iq}_{tag}"]) < tol, (iq, tag)
+
+
+@pytest.mark.parametrize("n,dtype", [(16, torch.complex128), (24, torch.complex128), (32, torch.complex64),
+                                     (48, torch.complex128), (48, torch.complex64), (40, torch.complex128)])
+def test_hpsi_batched_against_oracle(n, dtype):
+    """Batched hpsi over states of both isospins on larger grids vs the oracle."""
+    import hfb
+    from oracle import model, meanfield as omf
+    rng = np.random.default_rng(n)
+    d = (0.8, 0.85, 0.9)
+    g = model.init_grids(n, n, n, *d)
+    x = [(np.arange(n) - (n - 1) / 2) * h for h in d]
+    r2 = x[0][:, None, None] ** 2 + x[1][None, :, None] ** 2 + x[2][None, None, :] ** 2
+    w = np.exp(-r2 / (0.05 * (n * d[0]) ** 2))
+    mfo = omf.init_meanfield(g)
+    mfo.upot = np.stack([-50 * w, -45 * w])
+    mfo.bmass = np.stack([20 + 2 * w, 21 + 1.5 * w])
+    mfo.v_pair = np.stack([-3 * w, -2 * w])
+    for k, s in (("aq", 0.3), ("spot", 0.2), ("wlspot", 1.0)):
+        setattr(mfo, k, s * rng.standard_normal((2, 3, 1, 1, 1)) * w[None, None])
+    ns, nn = 5, 3
+    psi = (rng.standard_normal((ns, 2, n, n, n)) + 1j * rng.standard_normal((ns, 2, n, n, n))) * w
+    wt = rng.uniform(0.2, 1.0, ns)
+    wu = rng.uniform(0.0, 0.5, ns)
+    p = hfb.params.init_params()
+    gg = hfb.grids.init_grids(p, nx=n, ny=n, nz=n, dx=d[0], dy=d[1], dz=d[2])
+    mf = hfb.meanfield.init_meanfield(gg, dtype)
+    for k in ("upot", "bmass", "v_pair", "aq", "spot", "wlspot"):
+        getattr(mf, k).copy_(T(getattr(mfo, k)))
+    mf.pack(dtype)
+    pt = T(psi, dtype)
+    out = torch.empty_like(pt)
+    omf_ = torch.empty_like(pt)
+    from hfb._lib import call, ptr, stream_ptr, prec_of
+    call("hfb_hpsi", gg.ctx.handle, prec_of(pt), ptr(mf.pot), ns, nn, ptr(pt), ptr(T(wt)), ptr(T(wu)), ptr(out),
+         ptr(omf_), None, stream_ptr())
+    tol = 1e-11 if dtype == torch.complex128 else 1e-4
+    for iq, sl in ((0, slice(0, nn)), (1, slice(nn, ns))):
+        r = omf.hpsi01(g, mfo, iq, wt[sl], wu[sl], psi[sl])
+        assert rel(out[sl], r[0]) < tol
+        assert rel(omf_[sl], r[1]) < tol
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_add_density_against_reference(unit, g8, dtype):
+    import hfb
+    tol = TOL64 if dtype == torch.complex128 else 1e-5
+    lv = hfb.levels.init_levels(g8, 3, 2, (4, 3), dtype=dtype)
+    lv.psi.copy_(T(unit["in_dens_psi"], dtype))
+    for k in ("wocc", "wguv", "pairwg", "wstates"):
+        getattr(lv, k).copy_(T(unit[f"in_dens_{k}"]))
+    d = hfb.densities.init_densities(g8)
+    hfb.densities.add_density(d, g8, lv)
+    for k in ("rho", "chi", "tau", "current", "sdens", "sodens"):
+        assert rel(getattr(d, k), unit[f"dens_{k}"]) < tol, k
+
+
+def test_kinetic_energy_against_reference(unit, g8):
+    import hfb
+    f = _forces8()
+    lv = hfb.levels.init_levels(g8, 3, 2, (4, 3))
+    lv.psi.copy_(T(unit["in_dens_psi"]))
+    hfb.inout.sp_properties(f, g8, lv)
+    assert rel(lv.sp_kinetic, unit["spp_sp_kinetic"]) < TOL64
+    # the fused path inside add_density gives the same numbers
+    for k in ("wocc", "wguv", "pairwg", "wstates"):
+        getattr(lv, k).copy_(T(unit[f"in_dens_{k}"]))
+    lv.sp_kinetic.zero_()
+    hfb.densities.add_density(hfb.densities.init_densities(g8), g8, lv, forces=f)
+    assert rel(lv.sp_kinetic, unit["spp_sp_kinetic"]) < TOL64
+
+
+def _dens_for_skyrme(g8, unit):
+    import hfb
+    d = hfb.densities.init_densities(g8)
+    for k in ("current", "sdens", "sodens"):
+        getattr(d, k).copy_(T(unit[f"dens_{k}"]))
+    for k in ("rho", "tau", "chi"):
+        getattr(d, k).copy_(T(unit[f"in_sky_{k}"]))
+    return d
+
+
+def test_skyrme_and_coulomb_against_reference(unit, g8):
+    import hfb
+    f = _forces8()
+    d = _dens_for_skyrme(g8, unit)
+    mf = hfb.meanfield.init_meanfield(g8)
+    c = hfb.coulomb.init_coulomb(g8)
+    st = type("S", (), {"outertype": "N"})()
+    hfb.meanfield.skyrme(c, d, f, g8, mf, hfb.params.init_params(), st)
+    for k in ("upot", "bmass", "divaq", "v_pair", "aq", "spot", "wlspot", "dbmass"):
+        assert rel(getattr(mf, k), unit[f"sky_{k}"]) < TOL64, k
+    assert abs(mf.ecorrp - float(unit["sky_ecorrp"])) <= 1e-11 * abs(float(unit["sky_ecorrp"]))
+    assert rel(c.wcoul, unit["sky_wcoul"]) < TOL64
+    w = hfb.coulomb.poisson(g8, None, c, d.rho)
+    assert rel(w, unit["sky_wcoul"]) < TOL64
+
+
+def test_energies_against_reference(unit, g8):
+    import hfb
+    f = _forces8()
+    d = _dens_for_skyrme(g8, unit)
+    mf = hfb.meanfield.init_meanfield(g8)
+    c = hfb.coulomb.init_coulomb(g8)
+    st = type("S", (), {"outertype": "N"})()
+    p = hfb.params.init_params()
+    hfb.meanfield.skyrme(c, d, f, g8, mf, p, st)
+    lv = hfb.levels.init_levels(g8, 3, 2, (4, 3))
+    lv.sp_energy.copy_(T(unit["in_en_sp_energy"]))
+    lv.sp_kinetic.copy_(T(unit["in_en_sp_kinetic"]))
+    for k in ("wocc", "wguv", "pairwg", "wstates"):
+        getattr(lv, k).copy_(T(unit[f"in_dens_{k}"]))
+    pr = hfb.pairs.Pairs()
+    pr.out[1] = torch.tensor([1.3, 0.7], dtype=torch.float64)
+    e = hfb.energies.init_energies()
+    hfb.energies.integ_energy(c, d, e, f, g8, lv, p, pr)
+    hfb.energies.sum_energy(e, lv, mf, pr, grids=g8)
+    e.sync()
+    for k in ("ehft", "ehf0", "ehf1", "ehf2", "ehf3", "ehfls", "ehflsodd", "ehfc", "ecorc", "ehfint", "e3corr",
+              "ehf", "tke", "ehfCrho0", "ehfCrho1", "ehfCdrho0", "ehfCdrho1", "ehfCtau0", "ehfCtau1", "ehfCdJ0",
+              "ehfCdJ1"):
+        ref = float(unit[f"en_{k}"])
+        assert abs(getattr(e, k) - ref) <= 1e-10 * max(abs(ref), 1.0), (k, getattr(e, k), ref)
+
+
+def test_bcs_against_reference(unit, g8):
+    import hfb
+    f = _forces8()
+    f.pair_cutoff = (5.0, 5.0)
+    f.state_cutoff = (20.0, 20.0)
+    lv = hfb.levels.init_levels(g8, 3, 2, (4, 3))
+    lv.sp_energy.copy_(T(unit["in_bcs_sp_energy"]))
+    lv.deltaf.copy_(T(unit["in_bcs_deltaf"]))
+    p = hfb.params.init_params()
+    p.iteration = 11
+    pr = hfb.pairs.Pairs()
+    pr.firstcall = False
+    hfb.pairs.pair(lv, None, f, p, g8, pr)
+    g8.ctx.check("pair")
+    for k in ("wocc", "wguv", "pairwg", "wstates", "deltaf"):
+        assert rel(getattr(lv, k), unit[f"bcs_{k}"]) < 1e-12, k
+    for k in ("eferm", "epair", "avdelt", "avdeltv2", "avg"):
+        assert rel(getattr(pr, k), unit[f"bcs_{k}"]) < 1e-12, k
+
+
+def test_bcs_not_bracketed_reports_status(g8):
+    """A particle number that no Fermi level on [-100, 100] reaches latches
+    HFB_ERR_NOT_BRACKETED (the reference's brentq raises)."""
+    import hfb
+    from hfb._lib import HfbError
+    f = _forces8()
+    lv = hfb.levels.init_levels(g8, 9, 2, (4, 3))       # 9 neutrons in 4 states
+    p = hfb.params.init_params()
+    p.iteration = 1
+    hfb.pairs.pair(lv, None, f, p, g8, hfb.pairs.Pairs())
+    with pytest.raises(HfbError) as e:
+        g8.ctx.check("pair")
+    assert e.value.code == 4
+
+
+@pytest.mark.parametrize("n", [7, 40, 96, 140])
+def test_eigh_jacobi(g8, n):
+    import hfb
+    from hfb._lib import call, ptr, stream_ptr
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a = a + a.conj().T
+    a[np.triu_indices(n, 1)] = 7.0 + 3.0j      # only the lower triangle may be read
+    al = np.tril(a) + np.tril(a, -1).conj().T
+    wref = np.linalg.eigvalsh(al)
+    at = T(a.astype(np.complex128))
+    w = torch.empty(n, dtype=torch.float64, device="cuda")
+    v = torch.empty((n, n), dtype=torch.complex128, device="cuda")
+    call("hfb_eigh", g8.ctx.handle, 1, n, n, ptr(at), ptr(w), ptr(v), stream_ptr())
+    g8.ctx.check("eigh")
+    wn, vn = w.cpu().numpy(), v.cpu().numpy()
+    assert np.max(np.abs(wn - wref)) < 1e-11 * np.max(np.abs(wref))
+    assert np.max(np.abs(vn.conj().T @ vn - np.eye(n))) < 1e-12
+    assert np.max(np.abs(vn.conj().T @ al @ vn - np.diag(wn))) < 1e-11 * np.max(np.abs(wref))
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_gram(dtype):
+    import hfb
+    from hfb._lib import call, ptr, stream_ptr, prec_of
+    n = 16
+    p = hfb.params.init_params()
+    g = hfb.grids.init_grids(p, nx=n, ny=n, nz=n, dx=1.0, dy=1.0, dz=1.0)
+    rng = np.random.default_rng(3)
+    ns = 37
+    K = 2 * n ** 3
+    a = rng.standard_normal((3, ns, K)) + 1j * rng.standard_normal((3, ns, K))
+    vp = rng.standard_normal(n ** 3)
+    out = torch.zeros((4, ns, ns), dtype=torch.complex128, device="cuda")
+    ta = [T(x, dtype) for x in a]
+    call("hfb_gram", g.ctx.handle, prec_of(ta[0]), 0, ns, 15, ptr(ta[0]), ptr(ta[1]), ptr(ta[2]), ptr(T(vp)), 0.5,
+         ptr(out), stream_ptr())
+    x3 = a[0] * np.tile(vp, 2)[None]
+    refs = [0.5 * a[0].conj() @ x.T for x in (a[0], a[1], a[2], x3)]
+    tol = 1e-12 if dtype == torch.complex128 else 2e-5
+    for k in range(4):
+        assert rel(out[k], refs[k]) < tol, k
