@@ -125,8 +125,9 @@ def test_hpsi_batched_against_oracle(n, dtype):
     pt = T(psi, dtype)
     out = torch.empty_like(pt)
     omf_ = torch.empty_like(pt)
+    wt_t, wu_t = T(wt), T(wu)          # keep the weight buffers alive across the launch
     from hfb._lib import call, ptr, stream_ptr, prec_of
-    call("hfb_hpsi", gg.ctx.handle, prec_of(pt), ptr(mf.pot), ns, nn, ptr(pt), ptr(T(wt)), ptr(T(wu)), ptr(out),
+    call("hfb_hpsi", gg.ctx.handle, prec_of(pt), ptr(mf.pot), ns, nn, ptr(pt), ptr(wt_t), ptr(wu_t), ptr(out),
          ptr(omf_), None, stream_ptr())
     tol = 1e-11 if dtype == torch.complex128 else 1e-4
     for iq, sl in ((0, slice(0, nn)), (1, slice(nn, ns))):
@@ -287,9 +288,11 @@ def test_gram(dtype):
     vp = rng.standard_normal(n ** 3)
     out = torch.zeros((4, ns, ns), dtype=torch.complex128, device="cuda")
     ta = [T(x, dtype) for x in a]
-    call("hfb_gram", g.ctx.handle, prec_of(ta[0]), 0, ns, 15, ptr(ta[0]), ptr(ta[1]), ptr(ta[2]), ptr(T(vp)), 0.5,
+    vpt = T(vp)
+    call("hfb_gram", g.ctx.handle, prec_of(ta[0]), 0, ns, 15, ptr(ta[0]), ptr(ta[1]), ptr(ta[2]), ptr(vpt), 0.5,
          ptr(out), stream_ptr())
     x3 = a[0] * np.tile(vp, 2)[None]
+    torch.cuda.synchronize()
     refs = [0.5 * a[0].conj() @ x.T for x in (a[0], a[1], a[2], x3)]
     tol = 1e-12 if dtype == torch.complex128 else 2e-5
     for k in range(4):
