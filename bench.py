@@ -1,0 +1,413 @@
+"""Benchmark: Pb208 HF-BCS time-to-converge, mixed FP32/FP64 vs plain FP64,
+on one B200, plus the hpsi HBM roofline.
+
+Workload (default): Pb208, N = 126, Z = 82, SLy4 + volume-delta pairing
+(60 MeV soft window), 48^3 grid at dx = 0.8 fm, 140 + 96 two-spinor states,
+harmonic-oscillator start, doubled-grid Coulomb; synthetic inputs only (the
+reference ships no data).  One "step" is one self-consistent iteration.
+
+  1. W warm-up iterations (FP32 and FP64) on a throwaway state.
+  2. FP64 run from the oscillator start until the geometric estimate of the
+     remaining energy change is below 0.05 keV: E_ref and the FP64
+     time-to-converge (first iteration after which |E - E_ref| <= 1 keV).
+  3. Mixed run through the public API (hfb.static.statichf_mixed): FP32
+     bulk, FP64 refinement tail.  Its time-to-converge is ``value``; the
+     same run timed with the host->device copy of the initial states from
+     pinned memory and the device->host read of the results is ``e2e``.
+  4. hpsi on all 236 states, timed with CUDA events on the launching stream:
+     algorithmic bytes (read psi, write h psi, potentials once per isospin)
+     per launch / launch time = roofline.achieved.
+  5. CPU baseline: the NumPy oracle (restatement of the reference) timed on a
+     bounded sample of one iteration, scaled to the iterations the FP64 run
+     needed.
+
+Multi-GPU: the path does not shard across GPUs in this build (replicas
+only): under torchrun every rank runs the same workload on its own GPU and
+the time is the maximum over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "jax-hfbfft_b200"))
+
+METRIC = "Pb208 time-to-converge (ΔE≤1keV) mixed vs FP64 on B200; hpsi HBM GB/s vs peak"
+UNIT = "s"
+FALLBACK_HBM_GBS = 6650.0
+# SCF iterations the FP64 run of this algorithm needs to reach 1 keV on
+# Pb208 (measured with this bench's FP64 leg); scales the reference arm's
+# per-iteration CPU sample to a time-to-converge.
+PB208_FP64_ITERS = 800
+# DRAM bytes per hpsi launch (both kernels, 236 FP32 states) from the ncu
+# capture summarised in profiles/hpsi_pb208_fp32.md; None until captured.
+HPSI_NCU_DRAM_BYTES = None
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _state(case_name, dtype):
+    from hfb import config
+    return config.setup(config.case_dict(case_name), dtype=dtype)
+
+
+def warmup(case_name, W):
+    import torch
+    from hfb import static
+    for dt in (torch.complex64, torch.complex128):
+        st = _state(case_name, dt)
+        S = {k: st[k] for k in static._STATE_KEYS}
+        static.prepare(**S)
+        for i in range(1, W + 1):
+            static.iterate(i, **S)
+    torch.cuda.synchronize()
+
+
+def converged_index(E, e_ref, tol, allowed):
+    """First index i (among ``allowed``) with |E[j] - e_ref| <= tol for every
+    j >= i in the run, or None."""
+    idx = None
+    for i in range(len(E) - 1, -1, -1):
+        if abs(E[i] - e_ref) > tol:
+            break
+        if allowed[i]:
+            idx = i
+    return idx
+
+
+def fp64_run(case_name, maxiter):
+    """Plain FP64 run with per-iteration CUDA events."""
+    import torch
+    from hfb import static
+    st = _state(case_name, torch.complex128)
+    S = {k: st[k] for k in static._STATE_KEYS}
+    ev0 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    static.prepare(**S)
+    evs, E = [], []
+    for i in range(1, maxiter + 1):
+        static.iterate(i, **S)
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        evs.append(e)
+        E.append(st["energies"].ehf)
+        rem = static.remaining_change(E)
+        if i > 60 and rem is not None and abs(rem) < 5e-5:
+            break
+    torch.cuda.synchronize()
+    t = [ev0.elapsed_time(e) / 1e3 for e in evs]
+    rem = static.remaining_change(E) or 0.0
+    return dict(E=E, t=t, e_ref=E[-1] + rem, iters=len(E), state=st)
+
+
+def mixed_e2e_run(case_name, maxiter):
+    """Mixed run through hfb.static.statichf_mixed.  The initial states are
+    copied from pinned host memory inside the timed region; E_bind, the
+    densities and the single-particle energies are read back at the end."""
+    import torch
+    from hfb import static, output
+    st = _state(case_name, torch.complex64)
+    host_psi = st["levels"].psi.cpu().pin_memory()
+    st["levels"].psi.zero_()
+    bytes_in = host_psi.numel() * host_psi.element_size()
+    evs, E, P = [], [], []
+    e_h2d0 = torch.cuda.Event(enable_timing=True)
+    e_h2d1 = torch.cuda.Event(enable_timing=True)
+    e_d2h0 = torch.cuda.Event(enable_timing=True)
+    e_d2h1 = torch.cuda.Event(enable_timing=True)
+
+    def on_it(i, e, prec):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        evs.append(ev)
+        E.append(e)
+        P.append(prec)
+
+    from hfb._lib import launch_count
+    n0 = launch_count()
+    torch.cuda.synchronize()
+    e_h2d0.record()
+    st["levels"].psi.copy_(host_psi, non_blocking=True)
+    e_h2d1.record()
+    hist, sw = static.statichf_mixed(st, maxiter=maxiter, on_iteration=on_it)
+    e_d2h0.record()
+    out_rho = st["densities"].rho.to("cpu", non_blocking=True)
+    out_spe = st["levels"].sp_energy.to("cpu", non_blocking=True)
+    out_e = torch.tensor([st["energies"].ehf])
+    e_d2h1.record()
+    torch.cuda.synchronize()
+    n1 = launch_count()
+    bytes_out = out_rho.numel() * 8 + out_spe.numel() * 8 + 8
+    t = [e_h2d1.elapsed_time(e) / 1e3 for e in evs]
+    return dict(E=E, t=t, P=P, switch=sw, iters=len(E), state=st, launches=n1 - n0,
+                h2d_s=e_h2d0.elapsed_time(e_h2d1) / 1e3, d2h_s=e_d2h0.elapsed_time(e_d2h1) / 1e3,
+                bytes_in=bytes_in, bytes_out=bytes_out)
+
+
+def hpsi_roofline(st, reps=20):
+    """Time hpsi over all states in FP32 on the converged state."""
+    import torch
+    from hfb._lib import call, ptr, stream_ptr, prec_of
+    lv, mf, g = st["levels"], st["meanfield"], st["grids"]
+    psi = lv.psi.to(torch.complex64).contiguous()
+    mf.pack(torch.complex64)
+    out = torch.empty_like(psi)
+    ns, nn = lv.nstmax, lv.npsi[0]
+    wt = torch.ones(ns, dtype=torch.float64, device="cuda")
+    wu = torch.zeros(ns, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def once():
+        call("hfb_hpsi", g.ctx.handle, prec_of(psi), ptr(mf.pot), ns, nn, ptr(psi), ptr(wt), ptr(wu), None, ptr(out),
+             None, stream_ptr())
+
+    for _ in range(3):
+        once()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        once()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    n3 = g.n3
+    bytes_alg = ns * 4 * n3 * 8 + 2 * 12 * n3 * 4
+    return t, bytes_alg
+
+
+def cpu_sample(case_name, nsub=16):
+    """One oracle (NumPy, FP64) self-consistent iteration of the workload on
+    the host: the per-state work (two hpsi, the preconditioner, the densities
+    and the kinetic energy) on ``nsub`` states scaled to all states; the
+    diagonalisation step, BCS, potentials, Coulomb and energies in full.
+    Returns (seconds per iteration, description)."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from hfb import config
+    from oracle import model, static as ost, meanfield as omf, densities as od, spectral, coulomb as oc
+    from oracle import energies as oe, pairs as op
+    case = config.case_dict(case_name)
+    g = model.init_grids(**case["grid"])
+    f = model.init_forces(**case["force"])
+    lvc = case["levels"]
+    lv = model.init_levels(g, lvc["nneut"], lvc["nprot"], tuple(lvc["npsi"]))
+    f, st = ost.init_static(f, lv, **case["static"])
+    lv = ost.harmosc(g, lv, st)
+    rs = ost.RunState(params=dict(mprint=1), forces=f, grids=g, levels=lv, mf=omf.init_meanfield(g),
+                      dens=od.init_densities(g), coulomb=oc.init_coulomb(g), st=st, en=oe.Energies(),
+                      pairs=op.Pairs())
+    sub = lv.psi[:nsub]
+    w = np.ones(nsub)
+    t0 = time.perf_counter()
+    for _ in range(2):
+        omf.hpsi01(g, rs.mf, 0, w, 0 * w, sub)
+    for k in range(nsub):
+        spectral.laplace(g, f.h2ma, 1.0, 0.0, sub[k], 0.0, 100.0)
+    od.state_contributions(w, w, sub, g.d)
+    np.fft.fftn(sub, axes=(2, 3, 4))
+    np.fft.ifftn(sub, axes=(2, 3, 4))
+    t_state = (time.perf_counter() - t0) / nsub
+    t1 = time.perf_counter()
+    rs.en, rs.levels, rs.st = ost.diagstep(rs.en, f, g, rs.levels, rs.st, True, True)
+    rs.dens.rho[:] = 0.08
+    rs.mf, rs.coulomb = omf.skyrme(rs.coulomb, rs.dens, f, g, rs.mf)
+    oe.integ_energy(rs.coulomb, rs.dens, rs.en, f, g, rs.levels, rs.pairs)
+    t_global = time.perf_counter() - t1
+    per_it = lv.nstmax * t_state + t_global
+    desc = (f"one {case_name} iteration of the NumPy oracle: per-state work timed on {nsub} of {lv.nstmax} states "
+            f"and scaled; diagonalisation, potentials, Coulomb and energies in full")
+    return per_it, desc
+
+
+def reference_arm(args, rank, world):
+    """The reference's CPU path on the host cores: the oracle port (JAX is not
+    installable here).  Each step is one bounded sample (cpu_sample); the
+    value scales the median per-iteration time to the FP64 iteration count."""
+    if rank != 0:
+        return None
+    k = max(args.steps, 1) if args.steps > 0 else 1
+    nsub = 16 if k + args.warmup <= 6 else 4
+    for _ in range(min(args.warmup, 1)):
+        cpu_sample(args.workload, nsub=2)
+    samples = []
+    desc = ""
+    for _ in range(k):
+        s, desc = cpu_sample(args.workload, nsub=nsub)
+        samples.append(s)
+    per_it = statistics.median(samples)
+    value = per_it * PB208_FP64_ITERS
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=len(samples), warmup=min(args.warmup, 1),
+                ms_per_step=per_it * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None, dtype="f64",
+                data="synthetic", impl="reference",
+                config=dict(workload=f"{args.workload} HF-BCS (the bench workload), FP64 NumPy oracle on host cores",
+                            iterations_assumed=PB208_FP64_ITERS),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=os.cpu_count(), kind="port",
+                                  sample=desc + f"; x {PB208_FP64_ITERS} iterations"),
+                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=0, help="max SCF iterations per run (0 = until converged)")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--workload", default="Pb208")
+    ap.add_argument("--tol-kev", type=float, default=1.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = reference_arm(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    maxiter = args.steps if args.steps > 0 else 4000
+    tol = args.tol_kev * 1e-3
+    warmup(args.workload, max(args.warmup, 3))
+    # FP64 reference run
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    r64 = fp64_run(args.workload, maxiter)
+    e_ref = r64["e_ref"]
+    i64 = converged_index(r64["E"], e_ref, tol, [True] * len(r64["E"]))
+    t64 = r64["t"][i64] if i64 is not None else None
+    # mixed run (the timed region of the headline number)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        rm = mixed_e2e_run(args.workload, maxiter)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    im = converged_index(rm["E"], e_ref, tol, [p == "f64" for p in rm["P"]])
+    tm = rm["t"][im] if im is not None else None
+    value = tm
+    if dist and value is not None:
+        v = torch.tensor([value, t64 or 0.0], device="cuda", dtype=torch.float64)
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        value, t64 = float(v[0]), float(v[1])
+    e2e = None if tm is None else rm["h2d_s"] + tm + rm["d2h_s"]
+    # hpsi roofline
+    t_h, b_h = hpsi_roofline(rm["state"])
+    peak, peak_kind = _peaks()
+    achieved = b_h / t_h / 1e9
+    from hfb.output import rms_radii
+    _, rms, _ = rms_radii(rm["state"]["densities"], rm["state"]["grids"])
+    line = dict(
+        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=im + 1 if im is not None else rm["iters"],
+        warmup=max(args.warmup, 3), ms_per_step=(value / (im + 1) * 1e3) if value else None, higher_is_better=False,
+        scaling="weak", vs_baseline=None, dtype="f32+f64", data="synthetic",
+        config=dict(workload=f"{args.workload} HF-BCS: SLy4 + volume-delta pairing, 48^3 grid dx 0.8 fm, "
+                             "140+96 2-spinor states, HO start, 96^3 Coulomb grid",
+                    parallelism="replicas" if world > 1 else "single GPU",
+                    l2="inputs larger than L2 (states 0.5-0.8 GB)", tolerance_kev=args.tol_kev,
+                    fp64_time_to_converge_s=t64, fp64_iterations=(i64 + 1) if i64 is not None else None,
+                    speedup_mixed_vs_fp64=(t64 / value) if (t64 and value) else None,
+                    mixed_iterations=(im + 1) if im is not None else None, mixed_switch_iteration=rm["switch"],
+                    e_ref_mev=e_ref, e_mixed_final_mev=rm["E"][-1],
+                    de_final_kev=abs(rm["E"][-1] - e_ref) * 1e3, rms_proton_fm=rms[1],
+                    fp64_ms_per_iteration=(r64["t"][-1] / r64["iters"] * 1e3)),
+        roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                      traffic=HPSI_NCU_DRAM_BYTES, kernel="hpsi (hpsi_xplane + hpsi_yplane), FP32, 236 states",
+                      launch_ms=t_h * 1e3, bytes_per_launch=b_h, peak_kind=peak_kind),
+        e2e=dict(value=e2e, unit=UNIT, h2d_bytes_per_step=rm["bytes_in"] / max(rm["iters"], 1),
+                 d2h_bytes_per_step=rm["bytes_out"] / max(rm["iters"], 1)),
+        gpu_launches=rm["launches"], clocks=clk.summary())
+    if rank == 0 and world == 1 and not args.no_cpu:
+        per_it, desc = cpu_sample(args.workload)
+        iters = (i64 + 1) if i64 is not None else PB208_FP64_ITERS
+        line["cpu_baseline"] = dict(value=per_it * iters, unit=UNIT, cores=os.cpu_count(), kind="port",
+                                    sample=desc + f"; x {iters} iterations")
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

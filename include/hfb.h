@@ -68,6 +68,8 @@ int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, double dz, int 
                    int nstmax, hfb_ctx_t* out);
 int hfb_ctx_destroy(hfb_ctx_t ctx);
 const char* hfb_status_string(int status);
+/* Number of kernels this library has launched in the process. */
+unsigned long long hfb_launch_count(void);
 /* Latched device-side status (synchronises the stream), then clears it. */
 int hfb_device_status(hfb_ctx_t ctx, void* stream, int* status_out);
 

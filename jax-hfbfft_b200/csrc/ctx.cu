@@ -3,10 +3,14 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <atomic>
 #include <vector>
 #include "hfb_ctx.cuh"
 
 namespace hfb {
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int coulomb_init(hfb_ctx_s* c);  // skyrme.cu
 
@@ -123,6 +127,8 @@ extern "C" int hfb_ctx_destroy(hfb_ctx_t c) {
   free(c);
   return HFB_OK;
 }
+
+extern "C" unsigned long long hfb_launch_count(void) { return hfb::g_launches.load(); }
 
 extern "C" const char* hfb_status_string(int s) {
   switch (s) {

@@ -171,22 +171,43 @@ struct JacRot {
 };
 
 constexpr int kJacMaxSweeps = 40;
+constexpr int kEighMax = 4;     // matrices per batched launch
+constexpr int kJacThreads = 1024;
+constexpr int kJacBlk = 4;      // 2x2 blocks per thread (half*(half+1)/2 <= 4096 -> n <= 180)
 
-// One CTA per matrix.  ``rot`` receives the rotations
-// [sweep][round][m/2]; ``nrounds_out`` the number of recorded rounds.
-__global__ void __launch_bounds__(1024)
-jacobi_kernel(int n, int lda, const double2* __restrict__ A, double* w, JacRot* rot, int* nrounds_out, int* status,
-              size_t rot_stride) {
+// One batched solve: up to kEighMax independent matrices, one CTA each.
+struct EighBatch {
+  int nb;
+  int n[kEighMax];
+  int lda[kEighMax];
+  const double2* a[kEighMax];
+  double* w[kEighMax];
+  double2* v[kEighMax];
+  int vblk0[kEighMax + 1];     // prefix of row blocks for the vector replay
+};
+
+// One CTA per matrix: cyclic two-sided Jacobi on the packed lower triangle.
+// Each round applies n/2 disjoint rotations (round-robin pairing); thread t
+// owns fixed 2x2 blocks (pair q1 rows x pair q2 columns, q1 >= q2) for the
+// whole solve, and skips a block when both of its rotations are the
+// identity.  Rotations are recorded for the eigenvector replay.
+__global__ void __launch_bounds__(kJacThreads)
+jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t rot_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int b = blockIdx.x;
+  const int n = eb.n[b], lda = eb.lda[b];
   const int m = n + (n & 1);   // pad odd sizes with a decoupled index
+  const int half = m / 2;
   double2* a = reinterpret_cast<double2*>(smem_raw);
   JacRot* rr = reinterpret_cast<JacRot*>(a + (size_t)m * (m + 1) / 2);
+  int* rp = reinterpret_cast<int*>(rr + half);
+  int* rq = rp + half;
+  int* act = rq + half;
   __shared__ int any_rot;
-  const double2* Ab = A + (size_t)b * n * lda;
+  const double2* Ab = eb.a[b];
   JacRot* rotb = rot + (size_t)b * rot_stride;
-  // load the lower triangle (eigh with symmetrize_input=False reads only it;
-  // the diagonal's imaginary part is ignored as by LAPACK zheevd)
+  // the lower triangle (eigh with symmetrize_input=False reads only it; the
+  // diagonal's imaginary part is ignored as by LAPACK heevd)
   for (int e = threadIdx.x; e < m * (m + 1) / 2; e += blockDim.x) {
     int k = (int)((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
     while (k * (k + 1) / 2 > e) --k;
@@ -197,15 +218,28 @@ jacobi_kernel(int n, int lda, const double2* __restrict__ A, double* w, JacRot* 
     if (k == l) v.y = 0.0;
     a[e] = v;
   }
+  // this thread's blocks (round independent)
+  const int nblk = half * (half + 1) / 2;
+  int bq1[kJacBlk], bq2[kJacBlk];
+#pragma unroll
+  for (int j = 0; j < kJacBlk; ++j) {
+    const int e = threadIdx.x + j * kJacThreads;
+    bq1[j] = bq2[j] = -1;
+    if (e < nblk) {
+      int q1 = (int)((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
+      while (q1 * (q1 + 1) / 2 > e) --q1;
+      while ((q1 + 1) * (q1 + 2) / 2 <= e) ++q1;
+      bq1[j] = q1;
+      bq2[j] = e - q1 * (q1 + 1) / 2;
+    }
+  }
   __syncthreads();
-  const int half = m / 2;
   int rounds = 0;
   int sweep = 0;
   for (; sweep < kJacMaxSweeps; ++sweep) {
     if (threadIdx.x == 0) any_rot = 0;
     __syncthreads();
     for (int r = 0; r < m - 1; ++r) {
-      // rotation parameters for each disjoint pair
       for (int q = threadIdx.x; q < half; q += blockDim.x) {
         int p_, q_;
         rr_pair(m, r, q, p_, q_);
@@ -214,8 +248,9 @@ jacobi_kernel(int n, int lda, const double2* __restrict__ A, double* w, JacRot* 
         const double app = a[pk(p_, p_)].x, aqq = a[pk(q_, q_)].x;
         const double2 apq = ld_h(a, p_, q_);
         const double mag = hypot(apq.x, apq.y);
-        // negligible off-diagonal element: relative to both diagonal entries
+        // negligible off-diagonal element relative to both diagonal entries
         const bool negl = (mag == 0.0) || (fabs(app) + 100.0 * mag == fabs(app) && fabs(aqq) + 100.0 * mag == fabs(aqq));
+        int on = 0;
         if (!negl) {
           const double theta = (aqq - app) / (2.0 * mag);
           double t = 1.0 / (fabs(theta) + sqrt(theta * theta + 1.0));
@@ -223,62 +258,64 @@ jacobi_kernel(int n, int lda, const double2* __restrict__ A, double* w, JacRot* 
           g.cs = 1.0 / sqrt(t * t + 1.0);
           g.sn = t * g.cs;
           g.om = make_double2(apq.x / mag, -apq.y / mag);
+          on = 1;
           any_rot = 1;
         }
         rr[q] = g;
+        rp[q] = p_;
+        rq[q] = q_;
+        act[q] = on;
+        rotb[(size_t)rounds * half + q] = g;
       }
       __syncthreads();
-      // 2x2 blocks (pair P1 rows, pair P2 cols), P1 >= P2: A' = G1^H B G2
-      const int nblk = half * (half + 1) / 2;
-      for (int e = threadIdx.x; e < nblk; e += blockDim.x) {
-        int q1 = (int)((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
-        while (q1 * (q1 + 1) / 2 > e) --q1;
-        while ((q1 + 1) * (q1 + 2) / 2 <= e) ++q1;
-        const int q2 = e - q1 * (q1 + 1) / 2;
-        const JacRot g1 = rr[q1], g2 = rr[q2];
-        int k0, k1, l0, l1;
-        rr_pair(m, r, q1, k0, k1);
-        rr_pair(m, r, q2, l0, l1);
+#pragma unroll
+      for (int j = 0; j < kJacBlk; ++j) {
+        const int q1 = bq1[j], q2 = bq2[j];
+        if (q1 < 0) continue;
+        const int a1 = act[q1], a2 = act[q2];
+        if (!a1 && !a2) continue;
+        const int k0 = rp[q1], k1 = rq[q1];
+        const JacRot g1 = rr[q1];
         if (q1 == q2) {
           const double app = a[pk(k0, k0)].x, aqq = a[pk(k1, k1)].x;
           const double2 apq = ld_h(a, k0, k1);
           const double mag = hypot(apq.x, apq.y);
-          if (g1.sn != 0.0) {
-            const double t = g1.sn / g1.cs;
-            a[pk(k0, k0)] = make_double2(app - t * mag, 0.0);
-            a[pk(k1, k1)] = make_double2(aqq + t * mag, 0.0);
-            st_h(a, k1, k0, make_double2(0.0, 0.0));
-          }
+          const double t = g1.sn / g1.cs;
+          a[pk(k0, k0)] = make_double2(app - t * mag, 0.0);
+          a[pk(k1, k1)] = make_double2(aqq + t * mag, 0.0);
+          st_h(a, k1, k0, make_double2(0.0, 0.0));
           continue;
         }
+        const int l0 = rp[q2], l1 = rq[q2];
+        const JacRot g2 = rr[q2];
         // G = [[cs, sn], [-sn om, cs om]] (rows: old index, cols: new index)
         double2 B00 = ld_h(a, k0, l0), B01 = ld_h(a, k0, l1), B10 = ld_h(a, k1, l0), B11 = ld_h(a, k1, l1);
-        // right multiply by G2: columns l0, l1
-        const double2 om2 = g2.om;
         auto cm = [](double2 x, double2 y) { return make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x); };
-        double2 t10 = cm(B01, om2), t11 = cm(B11, om2);
-        double2 C00 = make_double2(g2.cs * B00.x - g2.sn * t10.x, g2.cs * B00.y - g2.sn * t10.y);
-        double2 C01 = make_double2(g2.sn * B00.x + g2.cs * t10.x, g2.sn * B00.y + g2.cs * t10.y);
-        double2 C10 = make_double2(g2.cs * B10.x - g2.sn * t11.x, g2.cs * B10.y - g2.sn * t11.y);
-        double2 C11 = make_double2(g2.sn * B10.x + g2.cs * t11.x, g2.sn * B10.y + g2.cs * t11.y);
-        // left multiply by G1^H: rows k0, k1; G1^H = [[cs, -sn conj(om)], [sn, cs conj(om)]]
-        const double2 oc = make_double2(g1.om.x, -g1.om.y);
-        double2 u0 = cm(C10, oc), u1 = cm(C11, oc);
-        double2 D00 = make_double2(g1.cs * C00.x - g1.sn * u0.x, g1.cs * C00.y - g1.sn * u0.y);
-        double2 D01 = make_double2(g1.cs * C01.x - g1.sn * u1.x, g1.cs * C01.y - g1.sn * u1.y);
-        double2 D10 = make_double2(g1.sn * C00.x + g1.cs * u0.x, g1.sn * C00.y + g1.cs * u0.y);
-        double2 D11 = make_double2(g1.sn * C01.x + g1.cs * u1.x, g1.sn * C01.y + g1.cs * u1.y);
-        st_h(a, k0, l0, D00);
-        st_h(a, k0, l1, D01);
-        st_h(a, k1, l0, D10);
-        st_h(a, k1, l1, D11);
+        if (a2) {   // right multiply by G2 (columns l0, l1)
+          const double2 t10 = cm(B01, g2.om), t11 = cm(B11, g2.om);
+          const double2 c00 = make_double2(g2.cs * B00.x - g2.sn * t10.x, g2.cs * B00.y - g2.sn * t10.y);
+          const double2 c01 = make_double2(g2.sn * B00.x + g2.cs * t10.x, g2.sn * B00.y + g2.cs * t10.y);
+          const double2 c10 = make_double2(g2.cs * B10.x - g2.sn * t11.x, g2.cs * B10.y - g2.sn * t11.y);
+          const double2 c11 = make_double2(g2.sn * B10.x + g2.cs * t11.x, g2.sn * B10.y + g2.cs * t11.y);
+          B00 = c00; B01 = c01; B10 = c10; B11 = c11;
+        }
+        if (a1) {   // left multiply by G1^H = [[cs, -sn conj(om)], [sn, cs conj(om)]] (rows k0, k1)
+          const double2 oc = make_double2(g1.om.x, -g1.om.y);
+          const double2 u0 = cm(B10, oc), u1 = cm(B11, oc);
+          const double2 d00 = make_double2(g1.cs * B00.x - g1.sn * u0.x, g1.cs * B00.y - g1.sn * u0.y);
+          const double2 d01 = make_double2(g1.cs * B01.x - g1.sn * u1.x, g1.cs * B01.y - g1.sn * u1.y);
+          const double2 d10 = make_double2(g1.sn * B00.x + g1.cs * u0.x, g1.sn * B00.y + g1.cs * u0.y);
+          const double2 d11 = make_double2(g1.sn * B01.x + g1.cs * u1.x, g1.sn * B01.y + g1.cs * u1.y);
+          B00 = d00; B01 = d01; B10 = d10; B11 = d11;
+        }
+        st_h(a, k0, l0, B00);
+        st_h(a, k0, l1, B01);
+        st_h(a, k1, l0, B10);
+        st_h(a, k1, l1, B11);
       }
-      // record the round for the eigenvector replay
-      for (int q = threadIdx.x; q < half; q += blockDim.x) rotb[(size_t)rounds * half + q] = rr[q];
       __syncthreads();
       ++rounds;
     }
-    __syncthreads();
     const int cont = any_rot;
     __syncthreads();
     if (!cont) break;
@@ -287,18 +324,21 @@ jacobi_kernel(int n, int lda, const double2* __restrict__ A, double* w, JacRot* 
     nrounds_out[b] = rounds;
     if (sweep >= kJacMaxSweeps) latch_error(status, HFB_ERR_NO_CONVERGENCE);
   }
-  for (int k = threadIdx.x; k < n; k += blockDim.x) w[(size_t)b * n + k] = a[pk(k, k)].x;
+  double* wb = eb.w[b];
+  for (int k = threadIdx.x; k < n; k += blockDim.x) wb[k] = a[pk(k, k)].x;
 }
 
-// Replay: V = I * G_1 * G_2 * ...; one CTA per (matrix, block of 8 rows);
-// then permute columns into ascending eigenvalue order.
+// Replay V = I G_1 G_2 ... onto blocks of 8 rows, then order the columns by
+// ascending eigenvalue (stable for ties).
 __global__ void __launch_bounds__(256)
-jacobi_vectors_kernel(int n, int lda, const JacRot* __restrict__ rot, const int* __restrict__ nrounds,
-                      const double* __restrict__ w, double2* V, size_t rot_stride) {
+jacobi_vectors_kernel(EighBatch eb, const JacRot* __restrict__ rot, const int* __restrict__ nrounds,
+                      size_t rot_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int RB = 8;
-  const int nb = (n + RB - 1) / RB;
-  const int b = blockIdx.x / nb, rb = blockIdx.x % nb;
+  int b = 0;
+  while (b + 1 < eb.nb && (int)blockIdx.x >= eb.vblk0[b + 1]) ++b;
+  const int rb = blockIdx.x - eb.vblk0[b];
+  const int n = eb.n[b], lda = eb.lda[b];
   const int m = n + (n & 1), half = m / 2;
   double2* v = reinterpret_cast<double2*>(smem_raw);   // [RB][m]
   int* order = reinterpret_cast<int*>(v + (size_t)RB * m);
@@ -325,8 +365,7 @@ jacobi_vectors_kernel(int n, int lda, const JacRot* __restrict__ rot, const int*
     }
     __syncthreads();
   }
-  // ascending order of eigenvalues (stable: ties keep index order)
-  const double* wb = w + (size_t)b * n;
+  const double* wb = eb.w[b];
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     int rank = 0;
     const double wj = wb[j];
@@ -337,17 +376,18 @@ jacobi_vectors_kernel(int n, int lda, const JacRot* __restrict__ rot, const int*
     order[rank] = j;
   }
   __syncthreads();
-  double2* Vb = V + (size_t)b * n * lda;
+  double2* Vb = eb.v[b];
   for (int e = threadIdx.x; e < RB * n; e += blockDim.x) {
     const int i = e / n, c = e % n;
     if (r0 + i < n) Vb[(size_t)(r0 + i) * lda + c] = v[i * m + order[c]];
   }
 }
 
-__global__ void sort_values_kernel(int n, int nb, double* w) {
+__global__ void sort_values_kernel(EighBatch eb) {
   const int b = blockIdx.x;
+  const int n = eb.n[b];
   extern __shared__ double tmpw[];
-  double* wb = w + (size_t)b * n;
+  double* wb = eb.w[b];
   for (int j = threadIdx.x; j < n; j += blockDim.x) tmpw[j] = wb[j];
   __syncthreads();
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -358,25 +398,53 @@ __global__ void sort_values_kernel(int n, int nb, double* w) {
   }
 }
 
-// nb matrices a[nb][n][lda] -> w[nb][n] ascending, v[nb][n][lda].
-int eigh_launch(hfb_ctx_s* c, int nb, int n, int lda, const double2* a, double* w, double2* v, cudaStream_t st) {
-  if (nb <= 0 || n <= 0) return HFB_OK;
-  const int m = n + (n & 1);
-  const size_t smem = sizeof(double2) * (size_t)m * (m + 1) / 2 + sizeof(JacRot) * (m / 2);
+// Batched Hermitian eigensolver over the matrices of ``eb`` (all concurrent).
+int eigh_batch(hfb_ctx_s* c, EighBatch eb, cudaStream_t st) {
+  if (eb.nb <= 0) return HFB_OK;
+  int mmax = 0, nmax = 0;
+  eb.vblk0[0] = 0;
+  for (int i = 0; i < eb.nb; ++i) {
+    if (eb.n[i] <= 0 || eb.lda[i] < eb.n[i]) return HFB_ERR_ARG;
+    const int m = eb.n[i] + (eb.n[i] & 1);
+    mmax = m > mmax ? m : mmax;
+    nmax = eb.n[i] > nmax ? eb.n[i] : nmax;
+    eb.vblk0[i + 1] = eb.vblk0[i] + (eb.n[i] + 7) / 8;
+  }
+  const int half = mmax / 2;
+  if (half * (half + 1) / 2 > kJacBlk * kJacThreads) return HFB_ERR_ARG;
+  const size_t smem = sizeof(double2) * (size_t)mmax * (mmax + 1) / 2 + (sizeof(JacRot) + 3 * sizeof(int)) * half;
   if (smem > 227 * 1024) return HFB_ERR_ARG;
-  const size_t rot_stride = (size_t)kJacMaxSweeps * (m - 1) * (m / 2);
-  char* buf = (char*)scratch(c, hfb_ctx_s::S_MAT, sizeof(JacRot) * rot_stride * nb + sizeof(int) * nb + 64);
+  const size_t rot_stride = (size_t)kJacMaxSweeps * (mmax - 1) * half;
+  char* buf = (char*)scratch(c, hfb_ctx_s::S_MAT, sizeof(JacRot) * rot_stride * eb.nb + sizeof(int) * kEighMax + 64);
   if (!buf) return HFB_ERR_ALLOC;
   JacRot* rot = (JacRot*)buf;
-  int* nr = (int*)(buf + sizeof(JacRot) * rot_stride * nb);
+  int* nr = (int*)(buf + sizeof(JacRot) * rot_stride * eb.nb);
   cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  jacobi_kernel<<<nb, 1024, smem, st>>>(n, lda, a, w, rot, nr, c->dev_status, rot_stride);
+  jacobi_kernel<<<eb.nb, kJacThreads, smem, st>>>(eb, rot, nr, c->dev_status, rot_stride);
   HFB_CHECK_LAUNCH();
-  const size_t smem2 = sizeof(double2) * 8 * m + sizeof(int) * m;
-  jacobi_vectors_kernel<<<nb * ((n + 7) / 8), 256, smem2, st>>>(n, lda, rot, nr, w, v, rot_stride);
+  const size_t smem2 = sizeof(double2) * 8 * mmax + sizeof(int) * mmax;
+  jacobi_vectors_kernel<<<eb.vblk0[eb.nb], 256, smem2, st>>>(eb, rot, nr, rot_stride);
   HFB_CHECK_LAUNCH();
-  sort_values_kernel<<<nb, 256, sizeof(double) * n, st>>>(n, nb, w);
+  sort_values_kernel<<<eb.nb, 256, sizeof(double) * nmax, st>>>(eb);
   HFB_CHECK_LAUNCH();
+  return HFB_OK;
+}
+
+// nb matrices a[nb][n][lda] -> w[nb][n] ascending, v[nb][n][lda].
+int eigh_launch(hfb_ctx_s* c, int nb, int n, int lda, const double2* a, double* w, double2* v, cudaStream_t st) {
+  for (int b0 = 0; b0 < nb; b0 += kEighMax) {
+    EighBatch eb{};
+    eb.nb = nb - b0 < kEighMax ? nb - b0 : kEighMax;
+    for (int i = 0; i < eb.nb; ++i) {
+      eb.n[i] = n;
+      eb.lda[i] = lda;
+      eb.a[i] = a + (size_t)(b0 + i) * n * lda;
+      eb.w[i] = w + (size_t)(b0 + i) * n;
+      eb.v[i] = v + (size_t)(b0 + i) * n * lda;
+    }
+    int r = eigh_batch(c, eb, st);
+    if (r) return r;
+  }
   return HFB_OK;
 }
 
@@ -660,22 +728,35 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
   }
   diag_real_kernel<<<2, 256, 0, st>>>(ld, nper, off, gm, 4 * sm, a->sp_norm);
   HFB_CHECK_LAUNCH();
-  // eigh(S) for both isospins (lower triangle)
+  // eigh of S (and of lambda when diagonalising) for both isospins in one
+  // batched launch: the solves are independent and run on separate SMs.
+  EighBatch eb{};
   for (int iq = 0; iq < 2; ++iq) {
-    r = eigh_launch(ctx, 1, nq[iq], ld, gm + (size_t)iq * 4 * sm, w + (size_t)iq * ld, V + (size_t)iq * sm, st);
-    if (r) return r;
+    eb.n[eb.nb] = nq[iq];
+    eb.lda[eb.nb] = ld;
+    eb.a[eb.nb] = gm + (size_t)iq * 4 * sm;
+    eb.w[eb.nb] = w + (size_t)iq * ld;
+    eb.v[eb.nb] = V + (size_t)iq * sm;
+    ++eb.nb;
   }
+  if (a->diagonalize) {
+    for (int iq = 0; iq < 2; ++iq) {
+      eb.n[eb.nb] = nq[iq];
+      eb.lda[eb.nb] = ld;
+      eb.a[eb.nb] = gm + (size_t)iq * 4 * sm + sm;
+      eb.w[eb.nb] = w + 2 * ld + (size_t)iq * ld;
+      eb.v[eb.nb] = Vl + (size_t)iq * sm;
+      ++eb.nb;
+    }
+  }
+  r = eigh_batch(ctx, eb, st);
+  if (r) return r;
   loewdin_scale_kernel<<<dim3(64, 2), 256, 0, st>>>(ld, nper, w, ld, V, T, sm);
   HFB_CHECK_LAUNCH();
   r = zgemm_small(ld, ld, 0, 1, T, sm, V, sm, Ur, sm, nper, 2, st);
   if (r) return r;
   double2* Uuse = Ur;
   if (a->diagonalize) {
-    for (int iq = 0; iq < 2; ++iq) {
-      r = eigh_launch(ctx, 1, nq[iq], ld, gm + (size_t)iq * 4 * sm + sm, w + 2 * ld + (size_t)iq * ld,
-                      Vl + (size_t)iq * sm, st);
-      if (r) return r;
-    }
     r = zgemm_small(ld, ld, 0, 0, Ur, sm, Vl, sm, U, sm, nper, 2, st);
     if (r) return r;
     Uuse = U;

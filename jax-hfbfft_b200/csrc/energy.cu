@@ -353,13 +353,17 @@ extern "C" int hfb_harmosc(hfb_ctx_t ctx, int prec, int nst, const int* qn, doub
   const double* d = ctx->d;
   if (prec == HFB_F64) {
     ho_fill_kernel<double><<<g1, 256, 0, st>>>(n, nst, qn, radinx, radiny, radinz, d[0], d[1], d[2], (double2*)psi);
+    HFB_CHECK_LAUNCH();
     ho_norm_kernel<double><<<nst, 256, 0, st>>>(n, (const double2*)psi, radinx, radiny, radinz, d[0], d[1], d[2],
                                                 ctx->wxyz, nrm, nrm + nst);
+    HFB_CHECK_LAUNCH();
     ho_scale_kernel<double><<<g2, 256, 0, st>>>(n, qn, nrm, nrm + nst, (double2*)psi);
   } else {
     ho_fill_kernel<float><<<g1, 256, 0, st>>>(n, nst, qn, radinx, radiny, radinz, d[0], d[1], d[2], (float2*)psi);
+    HFB_CHECK_LAUNCH();
     ho_norm_kernel<float><<<nst, 256, 0, st>>>(n, (const float2*)psi, radinx, radiny, radinz, d[0], d[1], d[2],
                                                ctx->wxyz, nrm, nrm + nst);
+    HFB_CHECK_LAUNCH();
     ho_scale_kernel<float><<<g2, 256, 0, st>>>(n, qn, nrm, nrm + nst, (float2*)psi);
   }
   HFB_CHECK_LAUNCH();

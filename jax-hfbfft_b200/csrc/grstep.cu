@@ -405,6 +405,7 @@ extern "C" int hfb_grstep(hfb_ctx_t ctx, int prec, const hfb_grstep_args* a, voi
                       ovl, st);
   if (r) return r;
   state_reduce_kernel<<<(ns + 127) / 128, 128, 0, st>>>(ns, n, ovl, 0, a->wxyz, spe_new);
+  HFB_CHECK_LAUNCH();
   state_reduce_kernel<<<(ns + 127) / 128, 128, 0, st>>>(ns, n, ovl, 1, a->wxyz, hexp);
   HFB_CHECK_LAUNCH();
   // 2) damped step

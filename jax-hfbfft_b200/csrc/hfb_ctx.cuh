@@ -28,8 +28,12 @@ void* scratch(hfb_ctx_s* c, int s, size_t bytes);
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Counts every kernel launch of the library (reported by hfb_launch_count).
+void count_launch();
+
 #define HFB_CHECK_LAUNCH()                                            \
   do {                                                                \
+    hfb::count_launch();                                              \
     cudaError_t e_ = cudaGetLastError();                              \
     if (e_ != cudaSuccess) return HFB_ERR_CUDA;                       \
   } while (0)

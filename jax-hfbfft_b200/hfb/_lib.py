@@ -86,7 +86,7 @@ _PROTOS = {
     "hfb_sum_energy": [vp, C.c_int] + [vp] * 6 + [vp, vp],
     "hfb_rms": [vp, vp, vp, vp],
 }
-SYMBOLS = tuple(_PROTOS) + ("hfb_status_string",)
+SYMBOLS = tuple(_PROTOS) + ("hfb_status_string", "hfb_launch_count")
 
 _lib = None
 
@@ -105,6 +105,8 @@ def load():
         f.restype = C.c_int
     lib.hfb_status_string.argtypes = [C.c_int]
     lib.hfb_status_string.restype = C.c_char_p
+    lib.hfb_launch_count.argtypes = []
+    lib.hfb_launch_count.restype = C.c_ulonglong
     _lib = lib
     return lib
 
@@ -132,6 +134,11 @@ def ptr(t):
     if not t.is_contiguous():
         raise ValueError("expected a contiguous tensor")
     return t.data_ptr()
+
+
+def launch_count():
+    """Kernels launched by libhfb in this process so far."""
+    return int(load().hfb_launch_count())
 
 
 def stream_ptr():

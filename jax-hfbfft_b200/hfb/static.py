@@ -282,3 +282,64 @@ def to_precision(state, dtype):
     state["levels"].to_precision(dtype)
     state["meanfield"].pack(dtype)
     return state
+
+
+def remaining_change(E, w=25):
+    """Geometric estimate of E_limit - E[-1] from the last 2w+1 energies
+    (ratio of successive w-iteration differences); None while the tail is
+    not yet geometric.  Used by the stopping and precision-switch rules."""
+    if len(E) < 2 * w + 1:
+        return None
+    d1 = E[-1] - E[-1 - w]
+    d0 = E[-1 - w] - E[-1 - 2 * w]
+    if d0 == 0.0:
+        return 0.0 if d1 == 0.0 else None
+    r = d1 / d0
+    if not (0.0 < r < 1.0):
+        return None
+    return d1 * r / (1.0 - r)
+
+
+_STATE_KEYS = ("coulomb", "densities", "energies", "forces", "grids", "levels", "meanfield", "params", "static",
+               "pairs")
+
+
+def statichf_mixed(state, maxiter=4000, switch_mev=5e-4, floor_mev=5e-5, stop_mev=5e-5, min_tail=3,
+                   on_iteration=None):
+    """Mixed-precision self-consistent loop on a state dict from
+    hfb.config.setup (states complex64 at entry): FP32 bulk iterations until
+    the estimated remaining energy change is below ``switch_mev`` (or the
+    last 25 energy changes stay below the FP32 noise floor ``floor_mev``),
+    then FP64 refinement until the estimated remaining change is below
+    ``stop_mev``.  ``on_iteration(i, ehf, precision)`` runs after each
+    iteration.  Returns (history, switch_iteration)."""
+    S = {k: state[k] for k in _STATE_KEYS}
+    prepare(**S)
+    S["energies"].sync()
+    E = [S["energies"].ehf]
+    hist = []
+    switched = state["levels"].psi.dtype == torch.complex128
+    switch_it = 0 if switched else None
+    tail = 0
+    for i in range(1, maxiter + 1):
+        iterate(i, **S)
+        e = S["energies"].ehf
+        E.append(e)
+        prec = "f64" if switched else "f32"
+        hist.append((i, e, prec))
+        if on_iteration is not None:
+            on_iteration(i, e, prec)
+        if not switched:
+            rem = remaining_change(E)
+            recent = [abs(E[k] - E[k - 1]) for k in range(max(1, len(E) - 25), len(E))]
+            if (rem is not None and abs(rem) < switch_mev) or (len(E) > 60 and max(recent) < floor_mev):
+                to_precision(state, torch.complex128)
+                switched = True
+                switch_it = i
+                E = [e]
+        else:
+            tail += 1
+            rem = remaining_change(E)
+            if tail >= min_tail and rem is not None and abs(rem) < stop_mev:
+                break
+    return hist, switch_it

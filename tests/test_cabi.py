@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "hfb.h")
 
 def _declared():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(hfb_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*|unsigned long long)\s+(hfb_\w+)\s*\(", txt, re.M)))
 
 
 @pytest.fixture(scope="module")
