@@ -7,6 +7,7 @@
 //     out = sum_t coef_t * D_t applied along axis_t to in_t      (t < 3)
 // so divergences, curls and Laplacians are single jobs and one launch runs
 // many jobs without write conflicts.
+#include <mutex>
 #include "hfb_ctx.cuh"
 
 namespace hfb {
@@ -444,5 +445,81 @@ extern "C" int hfb_skyrme(hfb_ctx_t ctx, const hfb_force* f, int tcoul, const do
                                                                           (float*)pot);
     HFB_CHECK_LAUNCH();
   }
+  return HFB_OK;
+}
+
+// --------------------------------------------- Poisson without allocation --
+// A second entry point for the Coulomb solve for callers that must not
+// allocate device memory when they call the library: code that is being
+// recorded into a CUDA graph (an allocation inside stream capture is not
+// part of the graph and breaks the capture), applications whose device
+// memory is entirely owned by their own pool allocator, and latency-critical
+// loops where an allocation and its implicit synchronisation would stall.
+// Its work buffer is a fixed array in the library's device image instead of
+// the context's growable scratch arena.
+namespace hfb {
+
+// Doubled-grid work buffer: 64^3 complex doubles (4 MiB), i.e. grids up to
+// 32^3 (non-periodic) or 64^3 (periodic).  Every GPU that loads the library
+// holds it until the process exits.
+constexpr int kNoAllocN2 = 64;
+static __device__ __align__(256) double2 g_poisson_noalloc[(size_t)kNoAllocN2 * kNoAllocN2 * kNoAllocN2];
+
+// Device address of g_poisson_noalloc per device ordinal, looked up on the
+// first call made on that device (the array's host-side name is only a
+// stand-in and must never be passed to a kernel).
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[64] = {nullptr};
+
+static int noalloc_buffer(double2** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HFB_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_poisson_noalloc) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return HFB_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = p;
+  }
+  *out = (double2*)g_noalloc_addr[dev];
+  return HFB_OK;
+}
+
+}  // namespace hfb
+
+extern "C" int hfb_poisson_noalloc(hfb_ctx_t ctx, const double* rho_p, double* wcoul, void* stream) {
+  using namespace hfb;
+  if (!ctx || !rho_p || !wcoul) return HFB_ERR_ARG;
+  const int n = ctx->n, n2 = ctx->n2;
+  if (n2 > kNoAllocN2) return HFB_ERR_UNSUPPORTED_GRID;   // work buffer too small for this grid
+  double2* a = nullptr;
+  int r = noalloc_buffer(&a);
+  if (r) return r;
+  cudaStream_t st = as_stream(stream);
+  const size_t tot = (size_t)n2 * n2 * n2;
+  // the load writes every element of the n2^3 region: the zero padding
+  // outside the density is re-established on each call
+  pois_load_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(a, n, n2, rho_p);
+  HFB_CHECK_LAUNCH();
+  const bool pruned = !ctx->periodic;
+  r = dispatch_n2(n2, [&](auto nn) -> int {
+    constexpr int N2 = decltype(nn)::value;
+    return coul_fft3<N2, -1>(a, n, pruned, st);
+  });
+  if (r) return r;
+  const double e2 = 1.4399784085965135;
+  const double fac = ctx->periodic ? 4.0 * kPi * e2 : e2 * ctx->wxyz;
+  pois_mul_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(a, ctx->coul_q, tot, fac, ctx->periodic);
+  HFB_CHECK_LAUNCH();
+  r = dispatch_n2(n2, [&](auto nn) -> int {
+    constexpr int N2 = decltype(nn)::value;
+    return coul_fft3<N2, +1>(a, n, pruned, st);
+  });
+  if (r) return r;
+  const size_t t3 = (size_t)n * n * n;
+  pois_store_kernel<<<(unsigned)((t3 + 255) / 256), 256, 0, st>>>(a, n, n2, 1.0 / (double)tot, wcoul);
+  HFB_CHECK_LAUNCH();
   return HFB_OK;
 }

@@ -73,6 +73,7 @@ _PROTOS = {
     "hfb_hpsi": [vp, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp],
     "hfb_skyrme": [vp, C.POINTER(HfbForce), C.c_int] + [vp] * 6 + [vp] * 8 + [vp, vp, C.c_int, vp, vp],
     "hfb_poisson": [vp, vp, vp, vp],
+    "hfb_poisson_noalloc": [vp, vp, vp, vp],
     "hfb_add_density": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_double] + [vp] * 6 +
                        [C.POINTER(C.c_double), vp, vp],
     "hfb_sp_kinetic": [vp, C.c_int, C.c_int, C.c_int, vp, C.POINTER(C.c_double), vp, vp],
