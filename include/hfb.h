@@ -196,15 +196,18 @@ int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, void* stream);
 /* Building blocks of diagstep, exported for tests:
  * C_a = wxyz * Psi^H X_a for a in the mask (bit0 X=psi, bit1 X=hampsi,
  * bit2 X=hmfpsi, bit3 X=v_pair*psi), states [s0, s0+ns), out complex
- * [4][ns][ns]. */
+ * [4][ns][ns].  Matrices 0, 2 and 3 are Hermitian in the iteration (one set
+ * of vectors; h psi and v_pair psi with h, v_pair Hermitian) and are
+ * computed on their upper triangle and mirrored. */
 int hfb_gram(hfb_ctx_t ctx, int prec, int s0, int ns, int mask, const void* psi,
              const void* hampsi, const void* hmfpsi, const double* v_pair_iq, double wxyz,
              double* out, void* stream);
 /* Hermitian eigensolver (cyclic Jacobi, FP64) on nb matrices a[nb][n][lda]
  * using their lower triangle; eigenvalues ascending in w[nb][n],
- * eigenvectors in the columns of v[nb][n][lda]. */
+ * eigenvectors in the columns of v[nb][n][lda]; sweeps (optional device
+ * int[nb]) receives the number of Jacobi sweeps each matrix took. */
 int hfb_eigh(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w, double* v,
-             void* stream);
+             int* sweeps, void* stream);
 
 /* ---- pairs.py ---------------------------------------------------------- */
 typedef struct hfb_pair_args {

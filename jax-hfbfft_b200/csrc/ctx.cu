@@ -98,6 +98,12 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     return HFB_ERR_ALLOC;
   }
   cudaMemset(c->dev_status, 0, sizeof(int));
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    c->side = nullptr;
+  }
   const size_t n2c = (size_t)c->n2 * c->n2 * c->n2;
   if (cudaMalloc(&c->coul_q, n2c * sizeof(double2)) != cudaSuccess) {
     hfb_ctx_destroy(c);
@@ -122,6 +128,11 @@ extern "C" int hfb_ctx_destroy(hfb_ctx_t c) {
   }
   if (c->coul_q) cudaFree(c->coul_q);
   if (c->dev_status) cudaFree(c->dev_status);
+  if (c->side) {
+    cudaStreamDestroy(c->side);
+    cudaEventDestroy(c->ev_fork);
+    cudaEventDestroy(c->ev_join);
+  }
   for (int s = 0; s < hfb_ctx_s::S_NSLOT; ++s)
     if (c->slot[s]) cudaFree(c->slot[s]);
   free(c);
@@ -137,7 +148,7 @@ extern "C" const char* hfb_status_string(int s) {
     case HFB_ERR_UNSUPPORTED_GRID: return "unsupported grid (cubic n in {8,16,24,32,40,48})";
     case HFB_ERR_CUDA: return "CUDA error";
     case HFB_ERR_NOT_BRACKETED: return "BCS particle number not bracketed on [-100, 100]";
-    case HFB_ERR_NO_CONVERGENCE: return "iteration limit reached (Jacobi / Brent)";
+    case HFB_ERR_NO_CONVERGENCE: return "iteration limit reached (Jacobi / Newton-Schulz / Brent)";
     case HFB_ERR_NONFINITE: return "non-finite value";
     case HFB_ERR_ALLOC: return "device allocation failed";
     default: return "unknown status";

@@ -16,127 +16,172 @@
 namespace hfb {
 
 // ================================================================ Gram ====
-constexpr int GT = 32;     // states per tile (both i and j)
-constexpr int GK = 16;     // k step staged in shared memory
+// C = wxyz Psi^H X for X in {psi, hampsi, hmfpsi, v_pair psi} (mask bits 0-3)
+// over K = 2 n^3.  Work is a list of 48 x 48 output tiles, one matrix per
+// tile; S, H and G are Hermitian (Gram matrices of one set of vectors, h
+// and v_pair Hermitian) so only tiles with ti <= tj are computed and the
+// reduction mirrors them.  Split-K partials are summed in a fixed order.
+// 48-state tiles keep the padding of the usual neutron/proton counts small
+// (140 -> 144, 96 -> 96); 192 threads (16 x 12) hold 4 x 3 outputs each.
+constexpr int GT = 48;        // tile edge (states)
+constexpr int GKS = 8;        // k per shared-memory stage
 constexpr int GCHUNK = 8192;  // k per split-K chunk
+constexpr int GTHREADS = 192;
+constexpr int kGramMaxTiles = 160;
 
-// part[chunk][a][i][j] (complex, unscaled); grid (tiles_i*tiles_j, nchunk)
+struct GramTile {
+  unsigned char b, a, ti, tj;   // block (isospin), matrix, tile row, tile column
+};
+struct GramJob {
+  int ntile;
+  GramTile t[kGramMaxTiles];
+  int s0[2], ns[2];              // state range of each block
+  const double* vp[2];           // v_pair for each block (X = v psi)
+  int herm_mask;                 // matrices computed on upper tiles only
+};
+
 template <class R>
-__global__ void __launch_bounds__(256)
-gram_kernel(int ns, int mask, size_t K, size_t n3, const cplx<R>* __restrict__ psi, const cplx<R>* __restrict__ hampsi,
-            const cplx<R>* __restrict__ hmfpsi, const double* __restrict__ vp, double2* part) {
+__global__ void __launch_bounds__(GTHREADS)
+gram_kernel(GramJob job, size_t K, size_t n3, const cplx<R>* __restrict__ psi, const cplx<R>* __restrict__ hampsi,
+            const cplx<R>* __restrict__ hmfpsi, double2* part, int nchunk) {
   using Z = cplx<R>;
-  __shared__ Z As[GK][GT + 1];
-  __shared__ Z Bs[4][GK][GT + 1];
-  const int ntj = (ns + GT - 1) / GT;
-  const int ti = blockIdx.x / ntj, tj = blockIdx.x % ntj;
-  const int i0 = ti * GT, j0 = tj * GT;
+  __shared__ Z As[2][GKS][GT + 1];
+  __shared__ Z Bs[2][GKS][GT + 1];
+  const GramTile tl = job.t[blockIdx.x];
+  const int b = tl.b, am = tl.a;
+  const int ns = job.ns[b];
+  const int i0 = tl.ti * GT, j0 = tl.tj * GT;
+  const cplx<R>* P = psi + (size_t)job.s0[b] * K;
+  const cplx<R>* X = am == 1 ? hampsi + (size_t)job.s0[b] * K : am == 2 ? hmfpsi + (size_t)job.s0[b] * K : P;
+  const double* vp = job.vp[b];
   const size_t k0 = (size_t)blockIdx.y * GCHUNK;
   const size_t k1 = min(K, k0 + GCHUNK);
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;   // 16 x 16 threads, 2 x 2 outputs each
-  R acc[4][2][2][2];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;   // rows ty + 12 u, columns tx + 16 v
+  R acc[4][3][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int u = 0; u < 4; ++u)
 #pragma unroll
-    for (int u = 0; u < 2; ++u)
+    for (int v = 0; v < 3; ++v) acc[u][v][0] = acc[u][v][1] = R(0);
+  // loader: 48 states x 8 k per operand = 384 elements, two per thread
+  auto load = [&](int buf, size_t kb) {
 #pragma unroll
-      for (int v = 0; v < 2; ++v) acc[a][u][v][0] = acc[a][u][v][1] = R(0);
-  const Z* X[3] = {psi, hampsi, hmfpsi};
-  for (size_t kb = k0; kb < k1; kb += GK) {
-    // stage: each thread loads 2 elements per operand (32 states x 16 k = 512)
-    for (int e = threadIdx.x; e < GT * GK; e += 256) {
-      const int s = e / GK, kk = e % GK;
+    for (int h = 0; h < 2; ++h) {
+      const int e = threadIdx.x + GTHREADS * h;
+      const int st_ = e / GKS, kk = e % GKS;
       const size_t k = kb + kk;
-      const bool ok_k = k < k1;
-      const int gi = i0 + s, gj = j0 + s;
-      As[kk][s] = (ok_k && gi < ns) ? psi[(size_t)gi * K + k] : czero<Z>();
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        if (!(mask & (1 << a))) continue;
-        Z v = czero<Z>();
-        if (ok_k && gj < ns) {
-          if (a < 3) v = X[a][(size_t)gj * K + k];
-          else v = (R)vp[k % n3] * psi[(size_t)gj * K + k];
-        }
-        Bs[a][kk][s] = v;
+      const bool okk = k < k1;
+      const int gi = i0 + st_, gj = j0 + st_;
+      As[buf][kk][st_] = (okk && gi < ns) ? P[(size_t)gi * K + k] : czero<Z>();
+      Z v = czero<Z>();
+      if (okk && gj < ns) {
+        v = X[(size_t)gj * K + k];
+        if (am == 3) v = (R)vp[k % n3] * v;
       }
+      Bs[buf][kk][st_] = v;
     }
-    __syncthreads();
+  };
+  load(0, k0);
+  __syncthreads();
+  int buf = 0;
+  for (size_t kb = k0; kb < k1; kb += GKS) {
+    if (kb + GKS < k1) load(buf ^ 1, kb + GKS);
 #pragma unroll
-    for (int kk = 0; kk < GK; ++kk) {
-      Z av[2];
-      av[0] = As[kk][ty];
-      av[1] = As[kk][ty + 16];
+    for (int kk = 0; kk < GKS; ++kk) {
+      Z av[4], bv[3];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        if (!(mask & (1 << a))) continue;
-        Z bv0 = Bs[a][kk][tx], bv1 = Bs[a][kk][tx + 16];
+      for (int u = 0; u < 4; ++u) av[u] = As[buf][kk][ty + 12 * u];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+      for (int v = 0; v < 3; ++v) bv[v] = Bs[buf][kk][tx + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
           // conj(a) * b
-          acc[a][u][0][0] += av[u].x * bv0.x + av[u].y * bv0.y;
-          acc[a][u][0][1] += av[u].x * bv0.y - av[u].y * bv0.x;
-          acc[a][u][1][0] += av[u].x * bv1.x + av[u].y * bv1.y;
-          acc[a][u][1][1] += av[u].x * bv1.y - av[u].y * bv1.x;
+          acc[u][v][0] += av[u].x * bv[v].x + av[u].y * bv[v].y;
+          acc[u][v][1] += av[u].x * bv[v].y - av[u].y * bv[v].x;
         }
-      }
     }
     __syncthreads();
+    buf ^= 1;
   }
-  const size_t stride = (size_t)ns * ns;
+  double2* o = part + ((size_t)blockIdx.x * nchunk + blockIdx.y) * GT * GT;
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    if (!(mask & (1 << a))) continue;
+  for (int u = 0; u < 4; ++u)
 #pragma unroll
-    for (int u = 0; u < 2; ++u)
-#pragma unroll
-      for (int v = 0; v < 2; ++v) {
-        const int gi = i0 + ty + 16 * u, gj = j0 + tx + 16 * v;
-        if (gi < ns && gj < ns)
-          part[((size_t)blockIdx.y * 4 + a) * stride + (size_t)gi * ns + gj] =
-              make_double2((double)acc[a][u][v][0], (double)acc[a][u][v][1]);
-      }
-  }
+    for (int v = 0; v < 3; ++v)
+      o[(ty + 12 * u) * GT + tx + 16 * v] = make_double2((double)acc[u][v][0], (double)acc[u][v][1]);
 }
 
-// out[a][i][j] (ld = ldo) = scale * sum_chunks part
-__global__ void gram_reduce_kernel(int ns, int mask, int nchunk, const double2* part, double scale, double2* out,
+struct GramOut {
+  double2* p[8];   // [block * 4 + matrix]
+};
+
+// out_a[b][i][j] = wxyz * sum over chunks (fixed order); Hermitian matrices
+// take the lower triangle from the upper one.
+__global__ void gram_reduce_kernel(GramJob job, int nchunk, const double2* part, double scale, GramOut outs,
                                    int ldo) {
-  const size_t stride = (size_t)ns * ns;
-  const size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  const int a = blockIdx.y;
-  if (e >= stride || !(mask & (1 << a))) return;
+  const int t = blockIdx.y;
+  const GramTile tl = job.t[t];
+  const int b = tl.b, am = tl.a;
+  const int ns = job.ns[b];
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= GT * GT) return;
+  const int li = e / GT, lj = e % GT;
+  const int i = tl.ti * GT + li, j = tl.tj * GT + lj;
+  if (i >= ns || j >= ns) return;
   double re = 0, im = 0;
+  const double2* p = part + (size_t)t * nchunk * GT * GT + e;
   for (int c = 0; c < nchunk; ++c) {
-    double2 v = part[((size_t)c * 4 + a) * stride + e];
+    const double2 v = p[(size_t)c * GT * GT];
     re += v.x;
     im += v.y;
   }
-  const int i = (int)(e / ns), j = (int)(e % ns);
-  out[(size_t)a * ldo * ldo + (size_t)i * ldo + j] = make_double2(scale * re, scale * im);
+  double2* out = outs.p[b * 4 + am];
+  const bool herm = (job.herm_mask >> am) & 1;
+  if (herm && i > j) return;           // written from the mirrored element below
+  out[(size_t)i * ldo + j] = make_double2(scale * re, scale * im);
+  if (herm && i != j) out[(size_t)j * ldo + i] = make_double2(scale * re, -scale * im);
 }
 
-int gram_launch(hfb_ctx_s* c, int prec, int s0, int ns, int mask, const void* psi, const void* hampsi,
-                const void* hmfpsi, const double* vp, double wxyz, double2* out, int ldo, cudaStream_t st) {
-  if (ns <= 0 || mask == 0) return HFB_OK;
+// One launch for the requested matrices of up to two state blocks.
+// outs[b * 4 + a] receives matrix a of block b (leading dimension ldo).
+int gram_launch(hfb_ctx_s* c, int prec, int nblk, const int* s0, const int* ns, const int* masks, const void* psi,
+                const void* hampsi, const void* hmfpsi, const double* const* vp, double wxyz, double2* const* outs_host,
+                int ldo, cudaStream_t st) {
   const size_t n3 = (size_t)c->n * c->n * c->n, K = 2 * n3;
   const int nchunk = (int)((K + GCHUNK - 1) / GCHUNK);
-  const int nt = (ns + GT - 1) / GT;
-  double2* part = (double2*)scratch(c, hfb_ctx_s::S_GRAM, sizeof(double2) * (size_t)nchunk * 4 * ns * ns);
+  GramJob job{};
+  job.herm_mask = 1 | 4 | 8;
+  for (int b = 0; b < nblk; ++b) {
+    job.s0[b] = s0[b];
+    job.ns[b] = ns[b];
+    job.vp[b] = vp ? vp[b] : nullptr;
+    const int nt = (ns[b] + GT - 1) / GT;
+    for (int a = 0; a < 4; ++a) {
+      if (!(masks[b] & (1 << a)) || ns[b] <= 0) continue;
+      const bool herm = (job.herm_mask >> a) & 1;
+      for (int ti = 0; ti < nt; ++ti)
+        for (int tj = herm ? ti : 0; tj < nt; ++tj) {
+          if (job.ntile >= kGramMaxTiles) return HFB_ERR_ARG;
+          job.t[job.ntile++] = GramTile{(unsigned char)b, (unsigned char)a, (unsigned char)ti, (unsigned char)tj};
+        }
+    }
+  }
+  if (job.ntile == 0) return HFB_OK;
+  double2* part = (double2*)scratch(c, hfb_ctx_s::S_GRAM, sizeof(double2) * (size_t)job.ntile * nchunk * GT * GT);
   if (!part) return HFB_ERR_ALLOC;
-  dim3 grid(nt * nt, nchunk);
-  const size_t off = (size_t)s0 * K;
+  GramOut ot;
+  for (int q = 0; q < 8; ++q) ot.p[q] = outs_host[q];
+  dim3 grid(job.ntile, nchunk);
   if (prec == HFB_F64)
-    gram_kernel<double><<<grid, 256, 0, st>>>(ns, mask, K, n3, (const double2*)psi + off,
-                                              hampsi ? (const double2*)hampsi + off : nullptr,
-                                              hmfpsi ? (const double2*)hmfpsi + off : nullptr, vp, part);
+    gram_kernel<double><<<grid, GTHREADS, 0, st>>>(job, K, n3, (const double2*)psi, (const double2*)hampsi,
+                                              (const double2*)hmfpsi, part, nchunk);
   else
-    gram_kernel<float><<<grid, 256, 0, st>>>(ns, mask, K, n3, (const float2*)psi + off,
-                                             hampsi ? (const float2*)hampsi + off : nullptr,
-                                             hmfpsi ? (const float2*)hmfpsi + off : nullptr, vp, part);
+    gram_kernel<float><<<grid, GTHREADS, 0, st>>>(job, K, n3, (const float2*)psi, (const float2*)hampsi,
+                                             (const float2*)hmfpsi, part, nchunk);
   HFB_CHECK_LAUNCH();
-  dim3 g2((unsigned)(((size_t)ns * ns + 255) / 256), 4);
-  gram_reduce_kernel<<<g2, 256, 0, st>>>(ns, mask, nchunk, part, wxyz, out, ldo);
+  dim3 g2((GT * GT + 255) / 256, job.ntile);
+  gram_reduce_kernel<<<g2, 256, 0, st>>>(job, nchunk, part, wxyz, ot, ldo);
   HFB_CHECK_LAUNCH();
   return HFB_OK;
 }
@@ -184,6 +229,7 @@ struct EighBatch {
   double* w[kEighMax];
   double2* v[kEighMax];
   int vblk0[kEighMax + 1];     // prefix of row blocks for the vector replay
+  int* sweeps;                 // optional device output [nb]: sweeps used
 };
 
 // One CTA per matrix: cyclic two-sided Jacobi on the packed lower triangle.
@@ -218,6 +264,36 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
     if (k == l) v.y = 0.0;
     a[e] = v;
   }
+  // Frobenius norm (invariant under the rotations): an off-diagonal element
+  // below eps ||A||_F is at the rounding-noise level the rotations
+  // themselves create, so it is not rotated (the eigenvalue error this
+  // leaves is second order in it)
+  __shared__ double red_f[32];
+  __shared__ double tol_abs;
+  {
+    double f2 = 0.0;
+    for (int e = threadIdx.x; e < m * (m + 1) / 2; e += blockDim.x) {
+      int k = (int)((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
+      while (k * (k + 1) / 2 > e) --k;
+      while ((k + 1) * (k + 2) / 2 <= e) ++k;
+      const int l = e - k * (k + 1) / 2;
+      double v = 0.0;
+      if (k < n && l < n) {
+        const double2 x = Ab[(size_t)k * lda + l];
+        v = (k == l ? x.x * x.x : 2.0 * (x.x * x.x + x.y * x.y));
+      }
+      f2 += v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+    if ((threadIdx.x & 31) == 0) red_f[threadIdx.x / 32] = f2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += red_f[w];
+      tol_abs = 2.220446049250313e-16 * sqrt(t);
+    }
+  }
   // this thread's blocks (round independent)
   const int nblk = half * (half + 1) / 2;
   int bq1[kJacBlk], bq2[kJacBlk];
@@ -249,7 +325,8 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
         const double2 apq = ld_h(a, p_, q_);
         const double mag = hypot(apq.x, apq.y);
         // negligible off-diagonal element relative to both diagonal entries
-        const bool negl = (mag == 0.0) || (fabs(app) + 100.0 * mag == fabs(app) && fabs(aqq) + 100.0 * mag == fabs(aqq));
+        const bool negl = (mag <= tol_abs) ||
+                          (fabs(app) + 100.0 * mag == fabs(app) && fabs(aqq) + 100.0 * mag == fabs(aqq));
         int on = 0;
         if (!negl) {
           const double theta = (aqq - app) / (2.0 * mag);
@@ -322,6 +399,7 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
   }
   if (threadIdx.x == 0) {
     nrounds_out[b] = rounds;
+    if (eb.sweeps) eb.sweeps[b] = sweep + 1;
     if (sweep >= kJacMaxSweeps) latch_error(status, HFB_ERR_NO_CONVERGENCE);
   }
   double* wb = eb.w[b];
@@ -431,9 +509,11 @@ int eigh_batch(hfb_ctx_s* c, EighBatch eb, cudaStream_t st) {
 }
 
 // nb matrices a[nb][n][lda] -> w[nb][n] ascending, v[nb][n][lda].
-int eigh_launch(hfb_ctx_s* c, int nb, int n, int lda, const double2* a, double* w, double2* v, cudaStream_t st) {
+int eigh_launch(hfb_ctx_s* c, int nb, int n, int lda, const double2* a, double* w, double2* v, int* sweeps,
+                cudaStream_t st) {
   for (int b0 = 0; b0 < nb; b0 += kEighMax) {
     EighBatch eb{};
+    eb.sweeps = sweeps ? sweeps + b0 : nullptr;
     eb.nb = nb - b0 < kEighMax ? nb - b0 : kEighMax;
     for (int i = 0; i < eb.nb; ++i) {
       eb.n[i] = n;
@@ -449,11 +529,15 @@ int eigh_launch(hfb_ctx_s* c, int nb, int n, int lda, const double2* a, double* 
 }
 
 // ========================================================= small GEMMs ====
-// C[b] = A'[b] B'[b] with A' = A or A^H, B' = B or B^H; n x n, leading dim ld.
-// Batched over blockIdx.z with per-batch strides (elements).
+// C[b] = alpha A'[b] B'[b] + dadd I with A' = A or A^H, B' = B or B^H;
+// n x n, leading dim ld, batched over blockIdx.z with per-batch strides.
+// When ``gate`` is given the kernel does nothing if gate_k > *gate (used to
+// retire converged Newton-Schulz steps without a host round trip).
 __global__ void zgemm_small_kernel(int n, int ld, int ta, int tb, const double2* A, size_t sa, const double2* B,
-                                   size_t sb, double2* C, size_t sc, Pair2 nper) {
+                                   size_t sb, double2* C, size_t sc, Pair2 nper, double alpha, double dadd,
+                                   const int* gate, int gate_k) {
   __shared__ double2 As[16][17], Bs[16][17];
+  if (gate && gate_k > *gate) return;
   const int b = blockIdx.z;
   const int nb = nper.v[b] > 0 ? nper.v[b] : n;
   const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
@@ -483,13 +567,128 @@ __global__ void zgemm_small_kernel(int n, int ld, int ta, int tb, const double2*
     }
     __syncthreads();
   }
-  if (i < nb && j < nb) C[b * sc + (size_t)i * ld + j] = make_double2(re, im);
+  if (i < nb && j < nb)
+    C[b * sc + (size_t)i * ld + j] = make_double2(alpha * re + (i == j ? dadd : 0.0), alpha * im);
 }
 
 static int zgemm_small(int nmax, int ld, int ta, int tb, const double2* A, size_t sa, const double2* B, size_t sb,
-                       double2* C, size_t sc, Pair2 nper, int batch, cudaStream_t st) {
+                       double2* C, size_t sc, Pair2 nper, int batch, cudaStream_t st, double alpha = 1.0,
+                       double dadd = 0.0, const int* gate = nullptr, int gate_k = 0) {
   dim3 grid((nmax + 15) / 16, (nmax + 15) / 16, batch);
-  zgemm_small_kernel<<<grid, dim3(16, 16), 0, st>>>(nmax, ld, ta, tb, A, sa, B, sb, C, sc, nper);
+  zgemm_small_kernel<<<grid, dim3(16, 16), 0, st>>>(nmax, ld, ta, tb, A, sa, B, sb, C, sc, nper, alpha, dadd, gate,
+                                                    gate_k);
+  HFB_CHECK_LAUNCH();
+  return HFB_OK;
+}
+
+// ------------------------------------------------- Loewdin by Newton-Schulz --
+// S^-1/2 from the coupled Newton-Schulz iteration on A = S / c, with c the
+// largest absolute row sum (so the spectrum of A lies in (0, 1]):
+//   T = (3 I - Z Y) / 2,  Y <- Y T,  Z <- T Z,   Y -> A^1/2, Z -> A^-1/2.
+// This is the matrix the reference forms as V diag(w^-1/2) V^H
+// (static.py:470-480) whenever no eigenvalue of S falls below its floor
+// max(1e-12, eps max(w) n); S is then positive definite with condition far
+// from that floor.  Steps after convergence are retired on the device.
+constexpr int kNSMaxIt = 24;
+
+// c_b and the start Y = S / c, Z = I; gate = large.
+__global__ void ns_init_kernel(int ld, Pair2 nper, const double2* S, size_t sS, double2* Y, double2* Z, size_t sm,
+                               double* cinv, int* gate) {
+  const int b = blockIdx.x;
+  const int n = nper.v[b];
+  const double2* Sb = S + b * sS;
+  __shared__ double red[32];
+  double mx = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double rs = 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double2 v = Sb[(size_t)i * ld + j];
+      rs += hypot(v.x, v.y);
+    }
+    mx = fmax(mx, rs);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) m = fmax(m, red[w]);
+    red[0] = m;
+    cinv[b] = 1.0 / m;
+    if (b == 0) *gate = 1 << 30;
+  }
+  __syncthreads();
+  const double ci = 1.0 / red[0];
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e / n, j = e % n;
+    const double2 v = Sb[(size_t)i * ld + j];
+    Y[b * sm + (size_t)i * ld + j] = make_double2(v.x * ci, v.y * ci);
+    Z[b * sm + (size_t)i * ld + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  }
+}
+
+// After T of step k: if max|T - I| over both blocks is below 1e-9, step k
+// is the last one applied (*gate = k); it squares that error to rounding.
+__global__ void ns_check_kernel(int ld, Pair2 nper, const double2* T, size_t sm, int* gate, int k) {
+  if (k > *gate) return;
+  __shared__ double red[32];
+  double mx = 0.0;
+  for (int b = 0; b < 2; ++b) {
+    const int n = nper.v[b];
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e / n, j = e % n;
+      const double2 v = T[b * sm + (size_t)i * ld + j];
+      mx = fmax(mx, hypot(v.x - (i == j ? 1.0 : 0.0), v.y));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) m = fmax(m, red[w]);
+    if (m < 1e-9) *gate = k;
+  }
+}
+
+// U = Z_final / sqrt(c); the result of step k sits in buffer (k + 1) % 2.
+__global__ void ns_final_kernel(int ld, Pair2 nper, const double2* Z0, const double2* Z1, size_t sm,
+                                const double* cinv, const int* gate, double2* U, int* status) {
+  const int b = blockIdx.y;
+  const int n = nper.v[b];
+  const int g = *gate;
+  const bool ok = g < kNSMaxIt;
+  const double2* Z = ((ok ? g : kNSMaxIt - 1) + 1) % 2 == 0 ? Z0 : Z1;
+  const double sc = sqrt(cinv[b]);
+  if (!ok && blockIdx.x == 0 && b == 0 && threadIdx.x == 0) latch_error(status, HFB_ERR_NO_CONVERGENCE);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += gridDim.x * blockDim.x) {
+    const int i = e / n, j = e % n;
+    const double2 v = Z[b * sm + (size_t)i * ld + j];
+    U[b * sm + (size_t)i * ld + j] = make_double2(v.x * sc, v.y * sc);
+  }
+}
+
+// Y0, Z0, Y1, Z1, T: work matrices [2][ld][ld] each; S: [2] with stride sS.
+static int loewdin_ns(hfb_ctx_s* c, int ld, Pair2 nper, const double2* S, size_t sS, double2* Y0, double2* Z0,
+                      double2* Y1, double2* Z1, double2* T, double* cinv, int* gate, double2* U, cudaStream_t st) {
+  const size_t sm = (size_t)ld * ld;
+  ns_init_kernel<<<2, 256, 0, st>>>(ld, nper, S, sS, Y0, Z0, sm, cinv, gate);
+  HFB_CHECK_LAUNCH();
+  int r;
+  for (int k = 0; k < kNSMaxIt; ++k) {
+    double2* Yc = (k % 2 == 0) ? Y0 : Y1;
+    double2* Zc = (k % 2 == 0) ? Z0 : Z1;
+    double2* Yn = (k % 2 == 0) ? Y1 : Y0;
+    double2* Zn = (k % 2 == 0) ? Z1 : Z0;
+    if ((r = zgemm_small(ld, ld, 0, 0, Zc, sm, Yc, sm, T, sm, nper, 2, st, -0.5, 1.5, gate, k))) return r;
+    ns_check_kernel<<<1, 1024, 0, st>>>(ld, nper, T, sm, gate, k);
+    HFB_CHECK_LAUNCH();
+    if ((r = zgemm_small(ld, ld, 0, 0, Yc, sm, T, sm, Yn, sm, nper, 2, st, 1.0, 0.0, gate, k))) return r;
+    if ((r = zgemm_small(ld, ld, 0, 0, T, sm, Zc, sm, Zn, sm, nper, 2, st, 1.0, 0.0, gate, k))) return r;
+  }
+  ns_final_kernel<<<dim3(32, 2), 256, 0, st>>>(ld, nper, Z0, Z1, sm, cinv, gate, U, c->dev_status);
   HFB_CHECK_LAUNCH();
   return HFB_OK;
 }
@@ -589,49 +788,56 @@ __global__ void copy_lambda_kernel(int ld, int nmax, Pair2 nper, const double2* 
 }
 
 // ============================================================== rotate ====
-// out1_j = sum_i psi_i U_ij, out2_j = sum_i psi_i L_ij for states of one
-// isospin block; tile 64 (k) x 32 (j) per CTA, 256 threads (8 outputs each).
+// out1_j = sum_i psi_i U_ij, out2_j = sum_i psi_i L_ij for the states of one
+// block: a (K x ns) by (ns x 2 ns) GEMM.  64 (k) x 64 (j) tile per CTA, 256
+// threads with 4 x 4 outputs each, double-buffered 8-state stages.
 template <class R>
 __global__ void __launch_bounds__(256)
 rotate_kernel(int ns, size_t K, const cplx<R>* __restrict__ psi, const double2* __restrict__ U,
               const double2* __restrict__ L, int ld, cplx<R>* out1, cplx<R>* out2) {
   using Z = cplx<R>;
-  constexpr int KT = 64, JT = 32, IT = 16;
-  __shared__ Z Ps[IT][KT + 1];
-  __shared__ Z Ws[IT][JT + 1];
+  constexpr int KT = 64, JT = 64, IT = 8;
+  __shared__ Z Ps[2][IT][KT + 1];
+  __shared__ Z Ws[2][IT][JT + 1];
   const int njt = (2 * ns + JT - 1) / JT;
   const int jt = blockIdx.x % njt;
   const size_t k0 = (size_t)(blockIdx.x / njt) * KT;
   const int j0 = jt * JT;
-  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;   // tx -> k rows (2), ty -> j columns (4)
-  R acc[2][4][2];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;   // tx -> k (4), ty -> j (4)
+  R acc[4][4][2];
 #pragma unroll
-  for (int u = 0; u < 2; ++u)
+  for (int u = 0; u < 4; ++u)
 #pragma unroll
     for (int v = 0; v < 4; ++v) acc[u][v][0] = acc[u][v][1] = R(0);
-  for (int i0 = 0; i0 < ns; i0 += IT) {
-    for (int e = threadIdx.x; e < IT * KT; e += 256) {
+  auto load = [&](int buf, int i0) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int e = threadIdx.x + 256 * h;
       const int ii = e / KT, kk = e % KT;
       const size_t k = k0 + kk;
-      Ps[ii][kk] = (i0 + ii < ns && k < K) ? psi[(size_t)(i0 + ii) * K + k] : czero<Z>();
-    }
-    for (int e = threadIdx.x; e < IT * JT; e += 256) {
-      const int ii = e / JT, jj = e % JT;
+      Ps[buf][ii][kk] = (i0 + ii < ns && k < K) ? psi[(size_t)(i0 + ii) * K + k] : czero<Z>();
+      const int ii2 = e / JT, jj = e % JT;
       const int j = j0 + jj;
-      double2 v = make_double2(0, 0);
-      if (i0 + ii < ns && j < 2 * ns) v = j < ns ? U[(size_t)(i0 + ii) * ld + j] : L[(size_t)(i0 + ii) * ld + (j - ns)];
-      Ws[ii][jj] = mk<R>((R)v.x, (R)v.y);
+      double2 w = make_double2(0, 0);
+      if (i0 + ii2 < ns && j < 2 * ns)
+        w = j < ns ? U[(size_t)(i0 + ii2) * ld + j] : L[(size_t)(i0 + ii2) * ld + (j - ns)];
+      Ws[buf][ii2][jj] = mk<R>((R)w.x, (R)w.y);
     }
-    __syncthreads();
+  };
+  load(0, 0);
+  __syncthreads();
+  int buf = 0;
+  for (int i0 = 0; i0 < ns; i0 += IT) {
+    if (i0 + IT < ns) load(buf ^ 1, i0 + IT);
 #pragma unroll
     for (int ii = 0; ii < IT; ++ii) {
-      Z pv[2], wv[4];
+      Z pv[4], wv[4];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) pv[u] = Ps[ii][tx + 32 * u];
+      for (int u = 0; u < 4; ++u) pv[u] = Ps[buf][ii][tx + 16 * u];
 #pragma unroll
-      for (int v = 0; v < 4; ++v) wv[v] = Ws[ii][ty + 8 * v];
+      for (int v = 0; v < 4; ++v) wv[v] = Ws[buf][ii][ty + 16 * v];
 #pragma unroll
-      for (int u = 0; u < 2; ++u)
+      for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
           acc[u][v][0] += pv[u].x * wv[v].x - pv[u].y * wv[v].y;
@@ -639,15 +845,16 @@ rotate_kernel(int ns, size_t K, const cplx<R>* __restrict__ psi, const double2* 
         }
     }
     __syncthreads();
+    buf ^= 1;
   }
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
-    const int j = j0 + ty + 8 * v;
+    const int j = j0 + ty + 16 * v;
     if (j >= 2 * ns) continue;
     Z* o = j < ns ? out1 + (size_t)j * K : out2 + (size_t)(j - ns) * K;
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const size_t k = k0 + tx + 32 * u;
+    for (int u = 0; u < 4; ++u) {
+      const size_t k = k0 + tx + 16 * u;
       if (k < K) o[k] = mk<R>(acc[u][v][0], acc[u][v][1]);
     }
   }
@@ -657,7 +864,7 @@ int rotate_launch(hfb_ctx_s* c, int prec, int s0, int ns, const void* psi, const
                   void* out1, void* out2, cudaStream_t st) {
   if (ns <= 0) return HFB_OK;
   const size_t K = (size_t)2 * c->n * c->n * c->n;
-  const int njt = (2 * ns + 31) / 32;
+  const int njt = (2 * ns + 63) / 64;
   const size_t nkt = (K + 63) / 64;
   const size_t off = (size_t)s0 * K;
   if (prec == HFB_F64)
@@ -678,13 +885,18 @@ extern "C" int hfb_gram(hfb_ctx_t ctx, int prec, int s0, int ns, int mask, const
                         const void* hmfpsi, const double* v_pair_iq, double wxyz, double* out, void* stream) {
   if (!ctx || !psi || !out || ns <= 0) return HFB_ERR_ARG;
   if (((mask & 2) && !hampsi) || ((mask & 4) && !hmfpsi) || ((mask & 8) && !v_pair_iq)) return HFB_ERR_ARG;
-  return gram_launch(ctx, prec, s0, ns, mask, psi, hampsi, hmfpsi, v_pair_iq, wxyz, (double2*)out, ns,
-                     as_stream(stream));
+  if ((ns + GT - 1) / GT > 255) return HFB_ERR_ARG;
+  double2* o = (double2*)out;
+  double2* outs[8] = {o, o + (size_t)ns * ns, o + 2 * (size_t)ns * ns, o + 3 * (size_t)ns * ns,
+                      nullptr, nullptr, nullptr, nullptr};
+  const double* vp[2] = {v_pair_iq, nullptr};
+  return gram_launch(ctx, prec, 1, &s0, &ns, &mask, psi, hampsi, hmfpsi, vp, wxyz, outs, ns, as_stream(stream));
 }
 
-extern "C" int hfb_eigh(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w, double* v, void* stream) {
+extern "C" int hfb_eigh(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w, double* v, int* sweeps,
+                        void* stream) {
   if (!ctx || !a || !w || !v || n <= 0 || lda < n) return HFB_ERR_ARG;
-  return eigh_launch(ctx, nb, n, lda, (const double2*)a, w, (double2*)v, as_stream(stream));
+  return eigh_launch(ctx, nb, n, lda, (const double2*)a, w, (double2*)v, sweeps, as_stream(stream));
 }
 
 extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, void* stream) {
@@ -698,48 +910,52 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
   const int ld = n0 > n1 ? n0 : n1;
   const size_t sm = (size_t)ld * ld;
   const size_t n3 = (size_t)ctx->n * ctx->n * ctx->n;
-  // workspace: 4 Gram matrices + 8 work matrices per isospin, eigenvalues, small ints
-  const size_t nmat = 2 * (4 + 8);
-  char* ws = (char*)scratch(ctx, hfb_ctx_s::S_SMALL, sizeof(double2) * nmat * sm + sizeof(double) * 4 * ld);
+  // workspace: 4 Gram matrices + 10 work matrices per isospin, eigenvalues,
+  // Newton-Schulz scalars
+  const size_t nmat = 2 * (4 + 10);
+  char* ws = (char*)scratch(ctx, hfb_ctx_s::S_SMALL,
+                            sizeof(double2) * nmat * sm + sizeof(double) * 4 * ld + 8 * sizeof(double));
   if (!ws) return HFB_ERR_ALLOC;
   double2* gm = (double2*)ws;                 // [iq][4][ld][ld]: S, Lambda, H_old, G_old
-  double2* V = gm + 2 * 4 * sm;               // [iq][ld][ld] eigenvectors of S
-  double2* T = V + 2 * sm;                    // scratch
+  double2* Y0 = gm + 2 * 4 * sm;              // Newton-Schulz work
+  double2* Z0 = Y0 + 2 * sm;
+  double2* Y1 = Z0 + 2 * sm;
+  double2* Z1 = Y1 + 2 * sm;
+  double2* T = Z1 + 2 * sm;                   // scratch
   double2* Ur = T + 2 * sm;                   // S^-1/2
   double2* Vl = Ur + 2 * sm;                  // eigenvectors of lambda
   double2* U = Vl + 2 * sm;                   // total transform
   double2* Hn = U + 2 * sm;                   // U^H H U
   double2* Gn = Hn + 2 * sm;                  // U^H G U
-  double2* Lw = Gn + 2 * sm;                  // U lambda
-  double* w = (double*)(Lw + 2 * sm);         // [iq][ld] (x2: S and lambda)
+  double2* Lw = Gn;                           // U lambda (Gn is dead by then)
+  double* w = (double*)(Gn + 2 * sm);         // [iq][ld] (x2: unused, lambda)
+  double* cinv = w + 4 * ld;
+  int* gate = (int*)(cinv + 4);
   Pair2 nper, off;
   nper.v[0] = n0; nper.v[1] = n1;
   off.v[0] = 0; off.v[1] = n0;
   const int nq[2] = {n0, n1}, so[2] = {0, n0};
   int r;
-  for (int iq = 0; iq < 2; ++iq) {
+  {
     int mask = 1;
     if (a->diagonalize) mask |= 2;
     if (a->construct) mask |= 4;
     if (a->construct && a->ipair) mask |= 8;
-    r = gram_launch(ctx, prec, so[iq], nq[iq], mask, a->psi, a->hampsi, a->hmfpsi,
-                    a->v_pair ? a->v_pair + (size_t)iq * n3 : nullptr, a->wxyz, gm + (size_t)iq * 4 * sm, ld, st);
+    const int masks[2] = {mask, mask};
+    const double* vp[2] = {a->v_pair, a->v_pair ? a->v_pair + n3 : nullptr};
+    double2* outs[8];
+    for (int iq = 0; iq < 2; ++iq)
+      for (int m = 0; m < 4; ++m) outs[iq * 4 + m] = gm + ((size_t)iq * 4 + m) * sm;
+    r = gram_launch(ctx, prec, 2, so, nq, masks, a->psi, a->hampsi, a->hmfpsi, vp, a->wxyz, outs, ld, st);
     if (r) return r;
   }
   diag_real_kernel<<<2, 256, 0, st>>>(ld, nper, off, gm, 4 * sm, a->sp_norm);
   HFB_CHECK_LAUNCH();
-  // eigh of S (and of lambda when diagonalising) for both isospins in one
-  // batched launch: the solves are independent and run on separate SMs.
-  EighBatch eb{};
-  for (int iq = 0; iq < 2; ++iq) {
-    eb.n[eb.nb] = nq[iq];
-    eb.lda[eb.nb] = ld;
-    eb.a[eb.nb] = gm + (size_t)iq * 4 * sm;
-    eb.w[eb.nb] = w + (size_t)iq * ld;
-    eb.v[eb.nb] = V + (size_t)iq * sm;
-    ++eb.nb;
-  }
+  // eigh of lambda (Jacobi, one CTA per isospin) on the side stream while the
+  // Newton-Schulz GEMMs for S^-1/2 run on the main stream
+  const bool fork = a->diagonalize && ctx->side;
   if (a->diagonalize) {
+    EighBatch eb{};
     for (int iq = 0; iq < 2; ++iq) {
       eb.n[eb.nb] = nq[iq];
       eb.lda[eb.nb] = ld;
@@ -748,15 +964,21 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
       eb.v[eb.nb] = Vl + (size_t)iq * sm;
       ++eb.nb;
     }
+    cudaStream_t es = st;
+    if (fork) {
+      cudaEventRecord(ctx->ev_fork, st);
+      cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
+      es = ctx->side;
+    }
+    r = eigh_batch(ctx, eb, es);
+    if (r) return r;
+    if (fork) cudaEventRecord(ctx->ev_join, ctx->side);
   }
-  r = eigh_batch(ctx, eb, st);
-  if (r) return r;
-  loewdin_scale_kernel<<<dim3(64, 2), 256, 0, st>>>(ld, nper, w, ld, V, T, sm);
-  HFB_CHECK_LAUNCH();
-  r = zgemm_small(ld, ld, 0, 1, T, sm, V, sm, Ur, sm, nper, 2, st);
+  r = loewdin_ns(ctx, ld, nper, gm, 4 * sm, Y0, Z0, Y1, Z1, T, cinv, gate, Ur, st);
   if (r) return r;
   double2* Uuse = Ur;
   if (a->diagonalize) {
+    if (fork) cudaStreamWaitEvent(st, ctx->ev_join, 0);
     r = zgemm_small(ld, ld, 0, 0, Ur, sm, Vl, sm, U, sm, nper, 2, st);
     if (r) return r;
     Uuse = U;

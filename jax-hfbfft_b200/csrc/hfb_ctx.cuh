@@ -15,6 +15,8 @@ struct hfb_ctx_s {
   double* der2[3];
   double2* coul_q;       // Green's function in k space, n2^3 (coulomb.py:23-52)
   int* dev_status;       // latched device-side error code
+  cudaStream_t side;     // secondary stream for independent work inside a call
+  cudaEvent_t ev_fork, ev_join;
   // scratch arena: fixed slots, grown on demand (never shrunk)
   enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_NSLOT };
   void* slot[S_NSLOT];

@@ -266,8 +266,10 @@ def test_eigh_jacobi(g8, n):
     at = T(a.astype(np.complex128))
     w = torch.empty(n, dtype=torch.float64, device="cuda")
     v = torch.empty((n, n), dtype=torch.complex128, device="cuda")
-    call("hfb_eigh", g8.ctx.handle, 1, n, n, ptr(at), ptr(w), ptr(v), stream_ptr())
+    sw = torch.zeros(1, dtype=torch.int32, device="cuda")
+    call("hfb_eigh", g8.ctx.handle, 1, n, n, ptr(at), ptr(w), ptr(v), ptr(sw), stream_ptr())
     g8.ctx.check("eigh")
+    assert 1 <= int(sw[0]) <= 15, int(sw[0])
     wn, vn = w.cpu().numpy(), v.cpu().numpy()
     assert np.max(np.abs(wn - wref)) < 1e-11 * np.max(np.abs(wref))
     assert np.max(np.abs(vn.conj().T @ vn - np.eye(n))) < 1e-12
@@ -285,6 +287,9 @@ def test_gram(dtype):
     ns = 37
     K = 2 * n ** 3
     a = rng.standard_normal((3, ns, K)) + 1j * rng.standard_normal((3, ns, K))
+    # the h psi slot holds a Hermitian operator applied to psi (here a real
+    # diagonal one), so its Gram matrix is Hermitian as in the iteration
+    a[2] = a[0] * rng.uniform(-2.0, 2.0, K)[None]
     vp = rng.standard_normal(n ** 3)
     out = torch.zeros((4, ns, ns), dtype=torch.complex128, device="cuda")
     ta = [T(x, dtype) for x in a]
