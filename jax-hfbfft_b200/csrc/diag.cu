@@ -230,6 +230,8 @@ struct EighBatch {
   double2* v[kEighMax];
   int vblk0[kEighMax + 1];     // prefix of row blocks for the vector replay
   int* sweeps;                 // optional device output [nb]: sweeps used
+  double tol_rel;              // off-diagonal threshold relative to ||A||_F (0: double eps)
+  int stage_half;              // rotations per round in the replay's staging buffer (set by eigh_batch)
 };
 
 // One CTA per matrix: cyclic two-sided Jacobi on the packed lower triangle.
@@ -291,7 +293,7 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
     if (threadIdx.x == 0) {
       double t = 0.0;
       for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += red_f[w];
-      tol_abs = 2.220446049250313e-16 * sqrt(t);
+      tol_abs = (eb.tol_rel > 0.0 ? eb.tol_rel : 2.220446049250313e-16) * sqrt(t);
     }
   }
   // this thread's blocks (round independent)
@@ -406,42 +408,76 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
   for (int k = threadIdx.x; k < n; k += blockDim.x) wb[k] = a[pk(k, k)].x;
 }
 
-// Replay V = I G_1 G_2 ... onto blocks of 8 rows, then order the columns by
-// ascending eigenvalue (stable for ties).
+// Replay V = I G_1 G_2 ... onto blocks of kVecRows rows, then order the
+// columns by ascending eigenvalue (stable for ties).  The recorded rotations
+// are streamed through shared memory kVecChunk rounds at a time with
+// cp.async double buffering, so each round costs one block barrier instead
+// of one global-memory latency.
+constexpr int kVecRows = 8;
+constexpr int kVecChunk = 8;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 __global__ void __launch_bounds__(256)
 jacobi_vectors_kernel(EighBatch eb, const JacRot* __restrict__ rot, const int* __restrict__ nrounds,
                       size_t rot_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int RB = 8;
   int b = 0;
   while (b + 1 < eb.nb && (int)blockIdx.x >= eb.vblk0[b + 1]) ++b;
   const int rb = blockIdx.x - eb.vblk0[b];
   const int n = eb.n[b], lda = eb.lda[b];
   const int m = n + (n & 1), half = m / 2;
-  double2* v = reinterpret_cast<double2*>(smem_raw);   // [RB][m]
-  int* order = reinterpret_cast<int*>(v + (size_t)RB * m);
-  const int r0 = rb * RB;
-  for (int e = threadIdx.x; e < RB * m; e += blockDim.x) {
+  JacRot* stage = reinterpret_cast<JacRot*>(smem_raw);                      // [2][kVecChunk][hmax]
+  const int hmax = eb.stage_half;
+  double2* v = reinterpret_cast<double2*>(stage + 2 * kVecChunk * hmax);    // [kVecRows][m]
+  int* order = reinterpret_cast<int*>(v + (size_t)kVecRows * m);
+  const int r0 = rb * kVecRows;
+  for (int e = threadIdx.x; e < kVecRows * m; e += blockDim.x) {
     const int i = e / m, j = e % m;
     v[e] = make_double2((r0 + i) == j ? 1.0 : 0.0, 0.0);
   }
-  __syncthreads();
   const JacRot* rb_ = rot + (size_t)b * rot_stride;
   const int nr = nrounds[b];
-  for (int r = 0; r < nr; ++r) {
-    const int rr_ = r % (m - 1);
-    for (int e = threadIdx.x; e < RB * half; e += blockDim.x) {
-      const int i = e / half, q = e % half;
-      const JacRot g = rb_[(size_t)r * half + q];
-      if (g.sn == 0.0) continue;
-      int p_, q_;
-      rr_pair(m, rr_, q, p_, q_);
-      const double2 vp = v[i * m + p_], vq = v[i * m + q_];
-      const double2 t = make_double2(vq.x * g.om.x - vq.y * g.om.y, vq.x * g.om.y + vq.y * g.om.x);
-      v[i * m + p_] = make_double2(g.cs * vp.x - g.sn * t.x, g.cs * vp.y - g.sn * t.y);
-      v[i * m + q_] = make_double2(g.sn * vp.x + g.cs * t.x, g.sn * vp.y + g.cs * t.y);
+  const int nchunk = (nr + kVecChunk - 1) / kVecChunk;
+  auto stage_load = [&](int c) {
+    if (c < nchunk) {
+      const int rs = c * kVecChunk;
+      const int cnt = (nr - rs < kVecChunk ? nr - rs : kVecChunk) * half;   // rotations in this chunk
+      const char* src = reinterpret_cast<const char*>(rb_ + (size_t)rs * half);
+      char* dst = reinterpret_cast<char*>(stage + (size_t)(c & 1) * kVecChunk * hmax);
+      for (int e = threadIdx.x; e < 2 * cnt; e += blockDim.x) cp_async16(dst + 16 * e, src + 16 * e);
     }
+    cp_async_commit();
+  };
+  stage_load(0);
+  for (int c = 0; c < nchunk; ++c) {
+    stage_load(c + 1);
+    cp_async_wait1();
     __syncthreads();
+    const JacRot* sg = stage + (size_t)(c & 1) * kVecChunk * hmax;
+    const int rs = c * kVecChunk;
+    const int re = nr - rs < kVecChunk ? nr : rs + kVecChunk;
+    for (int r = rs; r < re; ++r) {
+      const int rr_ = r % (m - 1);
+      const JacRot* gr = sg + (size_t)(r - rs) * half;
+      for (int e = threadIdx.x; e < kVecRows * half; e += blockDim.x) {
+        const int i = e / half, q = e % half;
+        const JacRot g = gr[q];
+        if (g.sn == 0.0) continue;
+        int p_, q_;
+        rr_pair(m, rr_, q, p_, q_);
+        const double2 vp = v[i * m + p_], vq = v[i * m + q_];
+        const double2 t = make_double2(vq.x * g.om.x - vq.y * g.om.y, vq.x * g.om.y + vq.y * g.om.x);
+        v[i * m + p_] = make_double2(g.cs * vp.x - g.sn * t.x, g.cs * vp.y - g.sn * t.y);
+        v[i * m + q_] = make_double2(g.sn * vp.x + g.cs * t.x, g.sn * vp.y + g.cs * t.y);
+      }
+      __syncthreads();
+    }
   }
   const double* wb = eb.w[b];
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -455,7 +491,7 @@ jacobi_vectors_kernel(EighBatch eb, const JacRot* __restrict__ rot, const int* _
   }
   __syncthreads();
   double2* Vb = eb.v[b];
-  for (int e = threadIdx.x; e < RB * n; e += blockDim.x) {
+  for (int e = threadIdx.x; e < kVecRows * n; e += blockDim.x) {
     const int i = e / n, c = e % n;
     if (r0 + i < n) Vb[(size_t)(r0 + i) * lda + c] = v[i * m + order[c]];
   }
@@ -486,7 +522,7 @@ int eigh_batch(hfb_ctx_s* c, EighBatch eb, cudaStream_t st) {
     const int m = eb.n[i] + (eb.n[i] & 1);
     mmax = m > mmax ? m : mmax;
     nmax = eb.n[i] > nmax ? eb.n[i] : nmax;
-    eb.vblk0[i + 1] = eb.vblk0[i] + (eb.n[i] + 7) / 8;
+    eb.vblk0[i + 1] = eb.vblk0[i] + (eb.n[i] + kVecRows - 1) / kVecRows;
   }
   const int half = mmax / 2;
   if (half * (half + 1) / 2 > kJacBlk * kJacThreads) return HFB_ERR_ARG;
@@ -500,7 +536,10 @@ int eigh_batch(hfb_ctx_s* c, EighBatch eb, cudaStream_t st) {
   cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   jacobi_kernel<<<eb.nb, kJacThreads, smem, st>>>(eb, rot, nr, c->dev_status, rot_stride);
   HFB_CHECK_LAUNCH();
-  const size_t smem2 = sizeof(double2) * 8 * mmax + sizeof(int) * mmax;
+  eb.stage_half = half;
+  const size_t smem2 =
+      sizeof(JacRot) * 2 * kVecChunk * half + sizeof(double2) * kVecRows * mmax + sizeof(int) * mmax;
+  cudaFuncSetAttribute(jacobi_vectors_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
   jacobi_vectors_kernel<<<eb.vblk0[eb.nb], 256, smem2, st>>>(eb, rot, nr, rot_stride);
   HFB_CHECK_LAUNCH();
   sort_values_kernel<<<eb.nb, 256, sizeof(double) * nmax, st>>>(eb);
@@ -956,6 +995,9 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
   const bool fork = a->diagonalize && ctx->side;
   if (a->diagonalize) {
     EighBatch eb{};
+    // single-precision states carry rounding noise of 2^-24 relative in
+    // lambda; rotating elements below that level refines nothing
+    if (prec != HFB_F64) eb.tol_rel = 5.9604644775390625e-08;
     for (int iq = 0; iq < 2; ++iq) {
       eb.n[eb.nb] = nq[iq];
       eb.lda[eb.nb] = ld;
