@@ -81,6 +81,10 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
   c->periodic = periodic ? 1 : 0;
   c->nstmax = nstmax;
   c->n2 = periodic ? nx : 2 * nx;
+  {
+    const char* e = getenv("HFB_NO_TCGEN05");
+    c->use_tcgen05 = (e && e[0] == '1') ? 0 : 1;
+  }
   const size_t nn = (size_t)nx * nx;
   for (int a = 0; a < 3; ++a) {
     std::vector<double> d1, d2;

@@ -143,11 +143,21 @@ __global__ void gram_reduce_kernel(GramJob job, int nchunk, const double2* part,
   if (herm && i != j) out[(size_t)j * ldo + i] = make_double2(scale * re, -scale * im);
 }
 
+int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const int* masks, const void* psi,
+                   const void* hampsi, const void* hmfpsi, const double* const* vp, double wxyz,
+                   double2* const* outs_host, int ldo, cudaStream_t st);   // gram_tc.cu
+
 // One launch for the requested matrices of up to two state blocks.
 // outs[b * 4 + a] receives matrix a of block b (leading dimension ldo).
+
 int gram_launch(hfb_ctx_s* c, int prec, int nblk, const int* s0, const int* ns, const int* masks, const void* psi,
                 const void* hampsi, const void* hmfpsi, const double* const* vp, double wxyz, double2* const* outs_host,
                 int ldo, cudaStream_t st) {
+  // single precision: tensor cores (three-term tf32) unless disabled for this context
+  if (prec != HFB_F64 && c->use_tcgen05) {
+    const int r = gram_tc_launch(c, nblk, s0, ns, masks, psi, hampsi, hmfpsi, vp, wxyz, outs_host, ldo, st);
+    if (r != HFB_ERR_UNSUPPORTED_GRID) return r;
+  }
   const size_t n3 = (size_t)c->n * c->n * c->n, K = 2 * n3;
   const int nchunk = (int)((K + GCHUNK - 1) / GCHUNK);
   GramJob job{};

@@ -16,6 +16,8 @@ struct hfb_ctx_s {
   double2* coul_q;       // Green's function in k space, n2^3 (coulomb.py:23-52)
   int* dev_status;       // latched device-side error code
   cudaStream_t side;     // secondary stream for independent work inside a call
+  int use_tcgen05;       // single-precision contractions on the tensor cores (default 1;
+                         // HFB_NO_TCGEN05=1 in the environment at creation selects CUDA cores)
   cudaEvent_t ev_fork, ev_join;
   // scratch arena: fixed slots, grown on demand (never shrunk)
   enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_NSLOT };

@@ -302,3 +302,60 @@ def test_gram(dtype):
     tol = 1e-12 if dtype == torch.complex128 else 2e-5
     for k in range(4):
         assert rel(out[k], refs[k]) < tol, k
+
+
+def _gram_case(n, s0, ns, seed):
+    import hfb
+    p = hfb.params.init_params()
+    g = hfb.grids.init_grids(p, nx=n, ny=n, nz=n, dx=1.0, dy=1.0, dz=1.0)
+    rng = np.random.default_rng(seed)
+    K = 2 * n ** 3
+    a = rng.standard_normal((3, s0 + ns, K)) + 1j * rng.standard_normal((3, s0 + ns, K))
+    a[2] = a[0] * rng.uniform(-2.0, 2.0, K)[None]
+    a = a.astype(np.complex64).astype(np.complex128)      # exact single-precision inputs
+    vp = rng.standard_normal(n ** 3).astype(np.float32).astype(np.float64)
+    return g, a, vp
+
+
+def _gram_run(g, a, vp, s0, ns, dtype):
+    from hfb._lib import call, ptr, stream_ptr, prec_of
+    out = torch.zeros((4, ns, ns), dtype=torch.complex128, device="cuda")
+    ta = [T(x, dtype) for x in a]
+    vpt = T(vp)
+    call("hfb_gram", g.ctx.handle, prec_of(ta[0]), s0, ns, 15, ptr(ta[0]), ptr(ta[1]), ptr(ta[2]), ptr(vpt), 0.5,
+         ptr(out), stream_ptr())
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,s0,ns", [(16, 0, 140), (16, 5, 96), (16, 3, 9), (24, 0, 70)])
+def test_gram_tensor_cores(n, s0, ns):
+    """Single-precision Gram on tcgen05 (three-term tf32, windowed fp32
+    accumulation, fp64 slice sums) against the fp64 Gram of the same
+    single-precision inputs: max error below 3e-6 of max |C|; the Hermitian
+    matrices' off-diagonal elements mirror exactly."""
+    g, a, vp = _gram_case(n, s0, ns, 11)
+    out = _gram_run(g, a, vp, s0, ns, torch.complex64)
+    sl = slice(s0, s0 + ns)
+    x3 = a[0][sl] * np.tile(vp, 2)[None]
+    refs = [0.5 * a[0][sl].conj() @ x.T for x in (a[0][sl], a[1][sl], a[2][sl], x3)]
+    for k in range(4):
+        assert rel(out[k], refs[k]) < 3e-6, (k, rel(out[k], refs[k]))
+    for k in (0, 2, 3):       # off-diagonal elements mirrored exactly
+        assert np.array_equal(np.triu(out[k], 1), np.triu(out[k].conj().T, 1)), k
+
+
+@pytest.mark.gpu
+def test_gram_tensor_cores_match_cuda_cores(monkeypatch):
+    """HFB_NO_TCGEN05=1 at context creation selects the CUDA-core kernel;
+    both single-precision paths agree to single-precision accuracy."""
+    n, s0, ns = 16, 2, 50
+    g, a, vp = _gram_case(n, s0, ns, 12)
+    tc = _gram_run(g, a, vp, s0, ns, torch.complex64)
+    monkeypatch.setenv("HFB_NO_TCGEN05", "1")
+    g2, _, _ = _gram_case(n, s0, ns, 12)
+    cc = _gram_run(g2, a, vp, s0, ns, torch.complex64)
+    for k in range(4):
+        assert rel(tc[k], cc[k]) < 1e-5, k
+        assert not np.array_equal(tc[k], cc[k]), k       # two different kernels ran
