@@ -45,10 +45,10 @@ FALLBACK_HBM_GBS = 6650.0
 # SCF iterations the FP64 run of this algorithm needs to reach 1 keV on
 # Pb208 (measured with this bench's FP64 leg); scales the reference arm's
 # per-iteration CPU sample to a time-to-converge.
-PB208_FP64_ITERS = 800
-# DRAM bytes per hpsi launch (both kernels, 236 FP32 states) from the ncu
-# capture summarised in profiles/hpsi_pb208_fp32.md; None until captured.
-HPSI_NCU_DRAM_BYTES = None
+PB208_FP64_ITERS = 675
+# DRAM bytes (read + write) per hpsi launch, both kernels, 236 FP32 states,
+# one output, from the ncu capture summarised in profiles/hpsi_pb208_fp32.md.
+HPSI_NCU_DRAM_BYTES = 426641664 + 376468224 + 839753216 + 373226752
 
 
 def _peaks():
