@@ -909,6 +909,107 @@ rotate_kernel(int ns, size_t K, const cplx<R>* __restrict__ psi, const double2* 
   }
 }
 
+// Single-precision variant with a larger register tile: 128 (k) x 96 (j)
+// per CTA, 256 threads holding 8 x 6 complex accumulators each (48
+// independent chains), 8 states per double-buffered shared-memory stage.
+// The 96-wide j tile keeps the padding of 2 ns columns small (280 -> 288,
+// 192 -> 192).
+constexpr int kRotKT = 128, kRotJT = 96, kRotIT = 8;
+
+__global__ void __launch_bounds__(256, 1)
+rotate_f32_kernel(int ns, size_t K, const float2* __restrict__ psi, const double2* __restrict__ U,
+                  const double2* __restrict__ L, int ld, float2* out1, float2* out2) {
+  __shared__ __align__(16) float2 Ps[2][kRotIT][kRotKT];
+  __shared__ __align__(16) float2 Ws[2][kRotIT][kRotJT];
+  const int njt = (2 * ns + kRotJT - 1) / kRotJT;
+  const int jt = blockIdx.x % njt;
+  const size_t k0 = (size_t)(blockIdx.x / njt) * kRotKT;
+  const int j0 = jt * kRotJT;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;   // k = tx + 16 u (u < 8), j = ty + 16 v (v < 6)
+  float acc[8][6][2];
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+#pragma unroll
+    for (int v = 0; v < 6; ++v) acc[u][v][0] = acc[u][v][1] = 0.f;
+  // stage loads into registers first so the next stage's global reads
+  // overlap this stage's arithmetic
+  float4 pr[2];
+  float2 wr[3];
+  auto fetch = [&](int i0) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int e = threadIdx.x + 256 * h;          // 512 float4 = 8 states x 64 pairs
+      const int ii = e / (kRotKT / 2), kk = 2 * (e % (kRotKT / 2));
+      const size_t k = k0 + kk;
+      pr[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (i0 + ii < ns && k < K) {
+        if (k + 2 <= K) pr[h] = *reinterpret_cast<const float4*>(psi + (size_t)(i0 + ii) * K + k);
+        else { const float2 a = psi[(size_t)(i0 + ii) * K + k]; pr[h] = make_float4(a.x, a.y, 0.f, 0.f); }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 3; ++h) {
+      const int e = threadIdx.x + 256 * h;          // 768 = 8 states x 96 columns
+      const int ii = e / kRotJT, jj = e % kRotJT;
+      const int j = j0 + jj;
+      double2 w = make_double2(0.0, 0.0);
+      if (i0 + ii < ns && j < 2 * ns)
+        w = j < ns ? U[(size_t)(i0 + ii) * ld + j] : L[(size_t)(i0 + ii) * ld + (j - ns)];
+      wr[h] = make_float2((float)w.x, (float)w.y);
+    }
+  };
+  auto stash = [&](int buf) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int e = threadIdx.x + 256 * h;
+      const int ii = e / (kRotKT / 2), kk = 2 * (e % (kRotKT / 2));
+      *reinterpret_cast<float4*>(&Ps[buf][ii][kk]) = pr[h];
+    }
+#pragma unroll
+    for (int h = 0; h < 3; ++h) {
+      const int e = threadIdx.x + 256 * h;
+      Ws[buf][e / kRotJT][e % kRotJT] = wr[h];
+    }
+  };
+  fetch(0);
+  stash(0);
+  __syncthreads();
+  int buf = 0;
+  for (int i0 = 0; i0 < ns; i0 += kRotIT) {
+    const bool more = i0 + kRotIT < ns;
+    if (more) fetch(i0 + kRotIT);
+#pragma unroll
+    for (int ii = 0; ii < kRotIT; ++ii) {
+      float2 pv[8], wv[6];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pv[u] = Ps[buf][ii][tx + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 6; ++v) wv[v] = Ws[buf][ii][ty + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int v = 0; v < 6; ++v) {
+          acc[u][v][0] = fmaf(pv[u].x, wv[v].x, fmaf(-pv[u].y, wv[v].y, acc[u][v][0]));
+          acc[u][v][1] = fmaf(pv[u].x, wv[v].y, fmaf(pv[u].y, wv[v].x, acc[u][v][1]));
+        }
+    }
+    if (more) stash(buf ^ 1);
+    __syncthreads();
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int v = 0; v < 6; ++v) {
+    const int j = j0 + ty + 16 * v;
+    if (j >= 2 * ns) continue;
+    float2* o = j < ns ? out1 + (size_t)j * K : out2 + (size_t)(j - ns) * K;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const size_t k = k0 + tx + 16 * u;
+      if (k < K) o[k] = make_float2(acc[u][v][0], acc[u][v][1]);
+    }
+  }
+}
+
 int rotate_launch(hfb_ctx_s* c, int prec, int s0, int ns, const void* psi, const double2* U, const double2* L, int ld,
                   void* out1, void* out2, cudaStream_t st) {
   if (ns <= 0) return HFB_OK;
@@ -919,9 +1020,12 @@ int rotate_launch(hfb_ctx_s* c, int prec, int s0, int ns, const void* psi, const
   if (prec == HFB_F64)
     rotate_kernel<double><<<(unsigned)(nkt * njt), 256, 0, st>>>(ns, K, (const double2*)psi + off, U, L, ld,
                                                                  (double2*)out1 + off, (double2*)out2 + off);
-  else
-    rotate_kernel<float><<<(unsigned)(nkt * njt), 256, 0, st>>>(ns, K, (const float2*)psi + off, U, L, ld,
-                                                                (float2*)out1 + off, (float2*)out2 + off);
+  else {
+    const int njt2 = (2 * ns + kRotJT - 1) / kRotJT;
+    const size_t nkt2 = (K + kRotKT - 1) / kRotKT;
+    rotate_f32_kernel<<<(unsigned)(nkt2 * njt2), 256, 0, st>>>(ns, K, (const float2*)psi + off, U, L, ld,
+                                                               (float2*)out1 + off, (float2*)out2 + off);
+  }
   HFB_CHECK_LAUNCH();
   return HFB_OK;
 }
