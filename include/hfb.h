@@ -245,6 +245,22 @@ int hfb_energies(hfb_ctx_t ctx, const hfb_force* f, int tcoul, double mass_numbe
 int hfb_sum_energy(hfb_ctx_t ctx, int nst, const double* wocc, const double* wstates,
                    const double* sp_kinetic, const double* sp_energy, const double* epair,
                    const double* ecorrp, double* out, void* stream);
+/* Explicit derivatives of the integrated functional ehfint (energies.py:
+ * 117-258) at fixed densities: out (device) receives HFB_NG doubles,
+ * dE/db for the coefficients b0, b0p, b1, b1p, b2, b2p, b3, b3p, b4, b4p
+ * (forces.py:95-107) and dE/dpower.  At a self-consistent solution the
+ * energy is stationary in the states and occupations, so these (chained
+ * with db/dt, db/dx, db/dW0) are the total derivatives of E_bind with
+ * respect to the Skyrme couplings: the adjoint of the fixed point vanishes
+ * for the energy itself.  No counterpart in the reference (its derivatives
+ * would come from jax.grad of the functional). */
+enum {
+  HFB_G_B0 = 0, HFB_G_B0P, HFB_G_B1, HFB_G_B1P, HFB_G_B2, HFB_G_B2P, HFB_G_B3, HFB_G_B3P,
+  HFB_G_B4, HFB_G_B4P, HFB_G_POWER, HFB_NG
+};
+int hfb_energy_grad(hfb_ctx_t ctx, const hfb_force* f, const double* rho, const double* tau,
+                    const double* current, const double* sdens, const double* sodens,
+                    double* out, void* stream);
 /* Point rms radii (output.py:187-226, 246): out[0..1] particle numbers,
  * out[2..3] rms per isospin, out[4] total rms. */
 int hfb_rms(hfb_ctx_t ctx, const double* rho, double* out, void* stream);

@@ -294,6 +294,74 @@ __global__ void ho_scale_kernel(int n, const int* qn, const double* norms, const
   p[i] = mk<R>((R)(p[i].x * sc), (R)(p[i].y * sc));
 }
 
+// ---------------------------------------------------------------------------
+// Explicit derivatives of the integrated Skyrme functional (energies.py:
+// 117-258, the terms of ehfint) with respect to its coefficients b0 .. b4p
+// and the density-dependence power alpha, at fixed densities.  Each term of
+// ehfint is linear in one b coefficient, so dE/db is the integral that
+// multiplies it; dE/dalpha = int rho^alpha ln(rho) (b3 rho^2 - b3p sum_q
+// rho_q^2) / 3 (points with rho = 0 contribute nothing).
+enum { G_B0 = 0, G_B0P, G_B1, G_B1P, G_B2, G_B2P, G_B3, G_B3P, G_B4, G_B4P, G_POWER, G_NSUM };
+static_assert(G_NSUM == HFB_NG, "gradient slots");
+
+__global__ void __launch_bounds__(256)
+energy_grad_points_kernel(hfb_force f, size_t n3, const double* rho, const double* tau, const double* sd,
+                          const double* dv, double* part) {
+  double acc[G_NSUM];
+#pragma unroll
+  for (int k = 0; k < G_NSUM; ++k) acc[k] = 0.0;
+  const double* d0 = dv;
+  const double* d1 = dv + (size_t)kNDerivE * n3;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
+    const double rn = rho[i], rp = rho[n3 + i];
+    const double rt = rn + rp, rq2 = rn * rn + rp * rp;
+    const double ln = d0[n3 + i], lp = d1[n3 + i];   // Laplacians
+    const double tn = tau[i], tp = tau[n3 + i];
+    const double jn = d0[i], jp = d1[i];             // div J
+    const double rtp = pow(rt, f.power);
+    acc[G_B0] += rt * rt / 2.0;
+    acc[G_B0P] += -rq2 / 2.0;
+    acc[G_B1] += rt * (tn + tp);
+    acc[G_B1P] += -(rn * tn + rp * tp);
+    acc[G_B2] += -rt * (ln + lp) / 2.0;
+    acc[G_B2P] += (rp * lp + rn * ln) / 2.0;
+    acc[G_B3] += rtp * rt * rt / 3.0;
+    acc[G_B3P] += -rtp * rq2 / 3.0;
+    double odd_b4 = 0.0, odd_b4p = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double cn = d0[(8 + k) * n3 + i], cp = d1[(8 + k) * n3 + i];   // curl j
+      const double sn = sd[(size_t)k * n3 + i], sp = sd[(size_t)(3 + k) * n3 + i];
+      odd_b4 += (sn + sp) * (cn + cp);
+      odd_b4p += sn * cn + sp * cp;
+    }
+    acc[G_B4] += -rt * (jn + jp) - odd_b4;
+    acc[G_B4P] += -(rp * jp + rn * jn) - odd_b4p;
+    if (rt > 0.0) acc[G_POWER] += rtp * log(rt) * (f.b3 * rt * rt - f.b3p * rq2) / 3.0;
+  }
+  __shared__ double red[G_NSUM][8];
+#pragma unroll
+  for (int k = 0; k < G_NSUM; ++k) {
+    double v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x % 32 == 0) red[k][threadIdx.x / 32] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < G_NSUM) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) v += red[threadIdx.x][w];
+    part[(size_t)blockIdx.x * G_NSUM + threadIdx.x] = v;
+  }
+}
+
+__global__ void energy_grad_final_kernel(double wxyz, int nblk, const double* part, double* out) {
+  if (threadIdx.x >= G_NSUM) return;
+  double v = 0.0;
+  for (int b = 0; b < nblk; ++b) v += part[(size_t)b * G_NSUM + threadIdx.x];
+  out[threadIdx.x] = wxyz * v;
+}
+
 }  // namespace hfb
 
 using namespace hfb;
@@ -366,6 +434,24 @@ extern "C" int hfb_harmosc(hfb_ctx_t ctx, int prec, int nst, const int* qn, doub
     HFB_CHECK_LAUNCH();
     ho_scale_kernel<float><<<g2, 256, 0, st>>>(n, qn, nrm, nrm + nst, (float2*)psi);
   }
+  HFB_CHECK_LAUNCH();
+  return HFB_OK;
+}
+
+extern "C" int hfb_energy_grad(hfb_ctx_t ctx, const hfb_force* f, const double* rho, const double* tau,
+                               const double* current, const double* sdens, const double* sodens, double* out,
+                               void* stream) {
+  if (!ctx || !f || !rho || !tau || !current || !sdens || !sodens || !out) return HFB_ERR_ARG;
+  cudaStream_t st = as_stream(stream);
+  const size_t n3 = (size_t)ctx->n * ctx->n * ctx->n;
+  double* dv = nullptr;
+  int r = density_derivatives(ctx, rho, current, sdens, sodens, false, &dv, st);
+  if (r) return r;
+  double* part = (double*)scratch(ctx, hfb_ctx_s::S_PART2, sizeof(double) * (size_t)kEnBlocks * G_NSUM);
+  if (!part) return HFB_ERR_ALLOC;
+  energy_grad_points_kernel<<<kEnBlocks, 256, 0, st>>>(*f, n3, rho, tau, sdens, dv, part);
+  HFB_CHECK_LAUNCH();
+  energy_grad_final_kernel<<<1, 32, 0, st>>>(ctx->wxyz, kEnBlocks, part, out);
   HFB_CHECK_LAUNCH();
   return HFB_OK;
 }

@@ -85,6 +85,7 @@ _PROTOS = {
     "hfb_pair": [vp, C.POINTER(PairArgs), vp],
     "hfb_energies": [vp, C.POINTER(HfbForce), C.c_int, C.c_double] + [vp] * 6 + [vp, vp, vp],
     "hfb_sum_energy": [vp, C.c_int] + [vp] * 6 + [vp, vp],
+    "hfb_energy_grad": [vp, C.POINTER(HfbForce)] + [vp] * 5 + [vp, vp],
     "hfb_rms": [vp, vp, vp, vp],
 }
 SYMBOLS = tuple(_PROTOS) + ("hfb_status_string", "hfb_launch_count")

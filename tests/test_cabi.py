@@ -115,3 +115,24 @@ def test_oscillator_radii():
     assert rz > rx and abs(rx * ry * rz - ho_radii(24, 24)[0] ** 3) < 1e-9
     c = case_dict("Pb208")
     assert c["levels"]["npsi"] == [140, 96] and c["grid"]["nx"] == 48
+
+
+def test_force_jacobian_matches_finite_differences():
+    """db/dtheta used by the energy sensitivities equals finite differences
+    of the coefficient formulas of init_forces."""
+    from hfb import adjoint
+    from hfb.forces import init_forces
+    base = init_forces(None, name="SLy4", ipair=5)
+    jac = adjoint._db_dtheta(base)
+    th0 = adjoint.theta_of(base)
+    for name, row in jac.items():
+        h = 1e-6 * abs(th0[name])
+        fp = init_forces(None, name="SLy4", ipair=5,
+                         overrides=adjoint.force_overrides(dict(force=dict(name="SLy4")),
+                                                           {name: th0[name] + h})["force"]["overrides"])
+        fm = init_forces(None, name="SLy4", ipair=5,
+                         overrides=adjoint.force_overrides(dict(force=dict(name="SLy4")),
+                                                           {name: th0[name] - h})["force"]["overrides"])
+        for b in ("b0", "b0p", "b1", "b1p", "b2", "b2p", "b3", "b3p", "b4", "b4p"):
+            d = (getattr(fp, b) - getattr(fm, b)) / (2 * h)
+            assert d == pytest.approx(row.get(b, 0.0), rel=1e-6, abs=1e-9), (name, b)
