@@ -3,30 +3,25 @@
 // C_a = wxyz Psi^H X_a (X = psi, hampsi, hmfpsi, v_pair psi; static.py:
 // 283-290, 380-387 and construct_hfb_matrices 484-577) for complex64 states.
 // The complex product is written as one real GEMM over the interleaved
-// (re, im) storage: a row of Psi~ holds (-im, re) per element, so for
-// states i, j   Re C_ij = Psi_i . X_j   and   Im C_ij = Psi~_i . X_j.
+// (re, im) storage: with A' = [Psi ; Psi~] (Psi~ row = (-im, re) per
+// element), D = A' X^T gives Re C in rows 0..n-1 and Im C in rows n..2n-1.
 // Operands are split as x = hi + lo with hi = tf32(x), lo = tf32(x - hi)
 // and D accumulates hi*hi + hi*lo + lo*hi (the three-term tf32 scheme,
 // about 22 significant bits per product).
 //
-// A unit is one matrix and one block of 64 states i: its 128 A rows are
-// Psi_i (rows 0-63) and Psi~_i (rows 64-127), its B rows the states j of X
-// from jlo on, where jlo = 0 for lambda and jlo = first i of the block for
-// the Hermitian S, H and G (only j >= i is needed; the reduction mirrors).
-// Each unit is split over K into slices, one CTA per slice:
-//   warps 0-6   load a 32-float K block of the rows from global memory
-//               (the next block's loads are in flight while the current one
-//               is split and stored), split it and store it into a
-//               128-byte-swizzled stage (3-stage ring);
-//   warp 7      issues the MMAs (M = 128, N = n - jlo padded to 16, K = 8)
-//               into one of two TMEM accumulators; each K block is a window
-//               that starts from zero;
+// One CTA owns one 128-row block of A' for one matrix and one slice of K:
+//   warps 0-6   load a 32-float K block of the rows from global memory,
+//               split it and store it into a 128-byte-swizzled stage
+//               (3-stage ring);
+//   warp 7      issues the MMAs (M = 128, N = n padded to 16, K = 8) into
+//               one of two TMEM accumulators; each K block is a window that
+//               starts from zero;
 //   warps 8-15  drain the finished accumulator into fp32 registers, so the
 //               tensor core's own fp32 accumulation spans at most one
 //               window (12 MMAs) and the sum over windows is rounded to
 //               nearest.
 // Per-slice partial sums are added in fp64 in a fixed order by a second
-// kernel, which also scatters the Re/Im rows into the complex outputs.
+// kernel, which also scatters Re/Im rows into the complex outputs.
 // Every wait is bounded; a timeout latches HFB_ERR_CUDA, drains the MMAs
 // in flight and releases TMEM before returning.
 #include <math.h>
@@ -52,19 +47,17 @@ constexpr uint32_t kTcABytes = 128 * 128;   // 128 rows x 128 bytes
 constexpr long long kTcWaitLimit = 2000000000LL;
 
 struct TcUnit {
-  unsigned char b, a, mb, pad;    // block (isospin), matrix, 64-state block
-  short cta0, nchunk;             // first CTA and number of K slices
-  short jlo, nn;                  // first column state, MMA N (multiple of 16)
+  unsigned char b, a, mb, pad;
 };
 struct TcJob {
-  int nunit, ncta, kb_total, n3;
+  int nunit, kchunks, kb_total, n3;
   TcUnit u[kTcMaxUnits];
   int s0[2], ns[2], np[2];
   const double* vp[2];
-  signed char unit_of[2][4][4];   // [block][matrix][64-state block] -> unit
+  signed char unit_of[2][4][4];   // [block][matrix][m-block] -> unit
 };
 
-__device__ __forceinline__ uint32_t stage_bytes(int nn) { return 2 * kTcABytes + 2 * (uint32_t)nn * 128; }
+__device__ __forceinline__ uint32_t stage_bytes(int np) { return 2 * kTcABytes + 2 * (uint32_t)np * 128; }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
 gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict__ hampsi,
@@ -75,17 +68,15 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
   __shared__ uint32_t tbase;
   __shared__ volatile int abort_flag;
 
-  int unit = 0;
-  while (unit + 1 < job.nunit && (int)blockIdx.x >= job.u[unit + 1].cta0) ++unit;
+  const int unit = blockIdx.x % job.nunit, chunk = blockIdx.x / job.nunit;
   const TcUnit U = job.u[unit];
-  const int chunk = (int)blockIdx.x - U.cta0;
   const int b = U.b, am = U.a, mb = U.mb;
-  const int n = job.ns[b], nn = U.nn, jlo = U.jlo;
+  const int n = job.ns[b], np = job.np[b];
   const size_t K = 2 * (size_t)job.n3;                 // complex elements per state
-  const int kb0 = (int)((long long)job.kb_total * chunk / U.nchunk);
-  const int kb1 = (int)((long long)job.kb_total * (chunk + 1) / U.nchunk);
+  const int kb0 = (int)((long long)job.kb_total * chunk / job.kchunks);
+  const int kb1 = (int)((long long)job.kb_total * (chunk + 1) / job.kchunks);
   const int nwin = kb1 - kb0;
-  const uint32_t sbytes = stage_bytes(nn);
+  const uint32_t sbytes = stage_bytes(np);
   const int tid = threadIdx.x, warp = tid / 32, lane = tid & 31;
 
   if (tid == 0) {
@@ -132,89 +123,78 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
     const int c = tid & 7;            // 16-byte chunk of the 128-byte row
     const int r0 = tid >> 3;          // first row; rows r0 + kTcRowsPerPass i
     const size_t rowf = 2 * K;        // floats per state
-    // A rows: state index (or -1); rows 64-127 are Psi~
+    // A' rows: state index (or -1) and whether the row is Psi~
     int rowA[kTcItemsA];
+    unsigned tmask = 0;
 #pragma unroll
     for (int i = 0; i < kTcItemsA; ++i) {
-      const int rl = r0 + kTcRowsPerPass * i;
-      const int st_ = mb * 64 + (rl & 63);
-      rowA[i] = (rl < 128 && st_ < n) ? st_ : -1;
+      const int rl = r0 + kTcRowsPerPass * i, rg = mb * 128 + rl;
+      rowA[i] = rl >= 128 ? -1 : rg < n ? rg : (rg < 2 * n ? rg - n : -1);
+      if (rg >= n && rg < 2 * n) tmask |= 1u << i;
     }
     const float* pa = psi + (size_t)job.s0[b] * rowf;
     const float* pb = (am == 1 ? hampsi : am == 2 ? hmfpsi : psi) + (size_t)job.s0[b] * rowf;
     const double* vp = job.vp[b];
-    auto load = [&](int w, float4 (&va)[kTcItemsA], float4 (&vb)[kTcItemsB]) {
+    for (int w = 0; w < nwin; ++w) {
+      const int s = w % kTcStages;
+      if (w >= kTcStages && !wait(&empty[s], (uint32_t)((w / kTcStages - 1) & 1))) break;
       const size_t off = (size_t)(kb0 + w) * 32 + 4 * c;
+      float4 va[kTcItemsA], vb[kTcItemsB];
 #pragma unroll
       for (int i = 0; i < kTcItemsA; ++i)
         if (rowA[i] >= 0) va[i] = __ldg(reinterpret_cast<const float4*>(pa + (size_t)rowA[i] * rowf + off));
 #pragma unroll
       for (int i = 0; i < kTcItemsB; ++i) {
-        const int r = r0 + kTcRowsPerPass * i, j = jlo + r;
-        if (r < nn && j < n) vb[i] = __ldg(reinterpret_cast<const float4*>(pb + (size_t)j * rowf + off));
+        const int j = r0 + kTcRowsPerPass * i;
+        if (j < n) vb[i] = __ldg(reinterpret_cast<const float4*>(pb + (size_t)j * rowf + off));
       }
-    };
-    auto put = [&](unsigned char* hi_base, uint32_t lo_delta, int row, float4 v) {
-      float4 h, l;
-      h.x = tc::to_tf32(v.x); l.x = tc::to_tf32(v.x - h.x);
-      h.y = tc::to_tf32(v.y); l.y = tc::to_tf32(v.y - h.y);
-      h.z = tc::to_tf32(v.z); l.z = tc::to_tf32(v.z - h.z);
-      h.w = tc::to_tf32(v.w); l.w = tc::to_tf32(v.w - h.w);
-      const uint32_t o = tc::sw128_offset(row, c);
-      *reinterpret_cast<float4*>(hi_base + o) = h;
-      *reinterpret_cast<float4*>(hi_base + lo_delta + o) = l;
-    };
-    auto store = [&](int w, const float4 (&va)[kTcItemsA], const float4 (&vb)[kTcItemsB]) -> bool {
-      const int s = w % kTcStages;
-      if (w >= kTcStages && !wait(&empty[s], (uint32_t)((w / kTcStages - 1) & 1))) return false;
       float v0 = 1.f, v1 = 1.f;
       if (am == 3) {
-        const size_t k = (((size_t)(kb0 + w) * 32 + 4 * c) / 2) % (size_t)job.n3;
+        const size_t k = (off / 2) % (size_t)job.n3;
         v0 = (float)vp[k];
         v1 = (float)vp[k + 1];
       }
       unsigned char* st = smem + (size_t)s * sbytes;
+      auto put = [&](unsigned char* hi_base, uint32_t lo_delta, int row, float4 v) {
+        float4 h, l;
+        h.x = tc::to_tf32(v.x); l.x = tc::to_tf32(v.x - h.x);
+        h.y = tc::to_tf32(v.y); l.y = tc::to_tf32(v.y - h.y);
+        h.z = tc::to_tf32(v.z); l.z = tc::to_tf32(v.z - h.z);
+        h.w = tc::to_tf32(v.w); l.w = tc::to_tf32(v.w - h.w);
+        const uint32_t o = tc::sw128_offset(row, c);
+        *reinterpret_cast<float4*>(hi_base + o) = h;
+        *reinterpret_cast<float4*>(hi_base + lo_delta + o) = l;
+      };
 #pragma unroll
       for (int i = 0; i < kTcItemsA; ++i) {
         if (rowA[i] < 0) continue;
-        const int rl = r0 + kTcRowsPerPass * i;
         float4 v = va[i];
-        if (rl >= 64) v = make_float4(-v.y, v.x, -v.w, v.z);
-        put(st, kTcABytes, rl, v);
+        if ((tmask >> i) & 1) v = make_float4(-v.y, v.x, -v.w, v.z);
+        put(st, kTcABytes, r0 + kTcRowsPerPass * i, v);
       }
 #pragma unroll
       for (int i = 0; i < kTcItemsB; ++i) {
-        const int r = r0 + kTcRowsPerPass * i;
-        if (r >= nn || jlo + r >= n) continue;
+        const int j = r0 + kTcRowsPerPass * i;
+        if (j >= n) continue;
         float4 v = vb[i];
         if (am == 3) v = make_float4(v0 * v.x, v0 * v.y, v1 * v.z, v1 * v.w);
-        put(st + 2 * kTcABytes, (uint32_t)nn * 128, r, v);
+        put(st + 2 * kTcABytes, (uint32_t)np * 128, j, v);
       }
       tc::fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&full[s]);
-      return true;
-    };
-    float4 a0[kTcItemsA], b0[kTcItemsB], a1[kTcItemsA], b1[kTcItemsB];
-    if (nwin > 0) load(0, a0, b0);
-    for (int w = 0; w < nwin; w += 2) {
-      if (w + 1 < nwin) load(w + 1, a1, b1);
-      if (!store(w, a0, b0)) break;
-      if (w + 1 >= nwin) break;
-      if (w + 2 < nwin) load(w + 2, a0, b0);
-      if (!store(w + 1, a1, b1)) break;
     }
   } else if (warp == kTcProducerWarps) {
     // ---------------------------------------------------------------- MMA
     if (lane == 0) {
-      const uint32_t idesc = tc::idesc_tf32(128, nn);
+      const uint32_t idesc = tc::idesc_tf32(128, np);
       for (int w = 0; w < nwin; ++w) {
         const int s = w % kTcStages, d = w & 1;
         if (!wait(&full[s], (uint32_t)((w / kTcStages) & 1))) break;
         if (w >= 2 && !wait(&dempty[d], (uint32_t)((w / 2 - 1) & 1))) break;
         tc::fence_after();
         const uint32_t sa = tc::smem_u32(smem + (size_t)s * sbytes);
-        const uint32_t ahi = sa, alo = sa + kTcABytes, bhi = sa + 2 * kTcABytes, blo = bhi + (uint32_t)nn * 128;
+        const uint32_t ahi = sa, alo = sa + kTcABytes, bhi = sa + 2 * kTcABytes, blo = bhi + (uint32_t)np * 128;
         const uint32_t dt = tmem + (uint32_t)(d * 256);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -234,7 +214,7 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
     // ----------------------------------------------------------- epilogue
     const int q = warp & 3;                       // TMEM lane quarter of this warp
     const int half = (warp - kTcProducerWarps - 1) / 4;   // two warps per quarter split the columns
-    const int ng = nn / 16, g0 = (ng + 1) / 2;
+    const int ng = np / 16, g0 = (ng + 1) / 2;
     const int gbeg = half ? g0 : 0, gcnt = half ? ng - g0 : g0;
     float acc[kTcMaxGroups][16];
 #pragma unroll
@@ -268,7 +248,7 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
         if (g < gcnt) {
 #pragma unroll
           for (int i = 0; i < 16; i += 4)
-            *reinterpret_cast<float4*>(o + jlo + (gbeg + g) * 16 + i) =
+            *reinterpret_cast<float4*>(o + (gbeg + g) * 16 + i) =
                 make_float4(acc[g][i], acc[g][i + 1], acc[g][i + 2], acc[g][i + 3]);
         }
     }
@@ -285,9 +265,9 @@ struct TcOut {
   double2* p[8];   // [block * 4 + matrix]
 };
 
-// out_a[b][i][j] = wxyz * (Re, Im) from rows i % 64 and 64 + i % 64 of the
-// unit of block i / 64, column j; the K slices are summed in fp64 in order.
-// Hermitian matrices mirror the upper triangle.
+// out_a[b][i][j] = wxyz * (Re, Im) from rows i and n + i of A' X^T, the
+// K slices summed in fp64 in order; Hermitian matrices mirror the upper
+// triangle.
 __global__ void gram_tc_reduce_kernel(TcJob job, const float* __restrict__ part, double scale, TcOut outs, int ldo,
                                       int bq, int aq) {
   const int b = bq, am = aq;
@@ -297,15 +277,12 @@ __global__ void gram_tc_reduce_kernel(TcJob job, const float* __restrict__ part,
   const int i = e / n, j = e % n;
   const bool herm = am != 1;
   if (herm && i > j) return;
-  const int mblk = i / 64;
-  const int ui = mblk == 0 ? job.unit_of[b][am][0] : mblk == 1 ? job.unit_of[b][am][1] : job.unit_of[b][am][2];
-  const TcUnit U = job.u[ui];
-  const int rre = i % 64, rim = 64 + i % 64;
+  const int rre = i, rim = n + i;
+  const int ure = job.unit_of[b][am][rre / 128], uim = job.unit_of[b][am][rim / 128];
   double re = 0.0, im = 0.0;
-  for (int c = 0; c < U.nchunk; ++c) {
-    const float* pc = part + (size_t)(U.cta0 + c) * 128 * kTcMaxNp;
-    re += (double)pc[(size_t)rre * kTcMaxNp + j];
-    im += (double)pc[(size_t)rim * kTcMaxNp + j];
+  for (int c = 0; c < job.kchunks; ++c) {
+    re += (double)part[(((size_t)c * job.nunit + ure) * 128 + (rre % 128)) * kTcMaxNp + j];
+    im += (double)part[(((size_t)c * job.nunit + uim) * 128 + (rim % 128)) * kTcMaxNp + j];
   }
   double2* out = outs.p[b * 4 + am];
   out[(size_t)i * ldo + j] = make_double2(scale * re, scale * im);
@@ -325,8 +302,6 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
   for (int b = 0; b < 2; ++b)
     for (int a = 0; a < 4; ++a)
       for (int m = 0; m < 4; ++m) job.unit_of[b][a][m] = -1;
-  int nnmax = 16;
-  long long wsum = 0;
   for (int b = 0; b < nblk; ++b) {
     if (ns[b] <= 0) continue;
     job.s0[b] = s0[b];
@@ -334,48 +309,36 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
     job.np[b] = (ns[b] + 15) / 16 * 16;
     job.vp[b] = vp ? vp[b] : nullptr;
     if (job.np[b] > kTcMaxNp) return HFB_ERR_UNSUPPORTED_GRID;
-    const int nmb = (ns[b] + 63) / 64;
+    const int nmb = (2 * ns[b] + 127) / 128;
     for (int a = 0; a < 4; ++a) {
       if (!(masks[b] & (1 << a))) continue;
       for (int m = 0; m < nmb; ++m) {
         if (job.nunit >= kTcMaxUnits) return HFB_ERR_UNSUPPORTED_GRID;
         job.unit_of[b][a][m] = (signed char)job.nunit;
-        TcUnit u{};
-        u.b = (unsigned char)b;
-        u.a = (unsigned char)a;
-        u.mb = (unsigned char)m;
-        u.jlo = (short)(a == 1 ? 0 : 64 * m);
-        u.nn = (short)(job.np[b] - u.jlo);
-        nnmax = u.nn > nnmax ? u.nn : nnmax;
-        wsum += 128 + u.nn;
-        job.u[job.nunit++] = u;
+        job.u[job.nunit++] = TcUnit{(unsigned char)b, (unsigned char)a, (unsigned char)m, 0};
       }
     }
   }
   if (job.nunit == 0) return HFB_OK;
-  // K slices per unit in proportion to its rows (128 A rows + nn B rows are
-  // loaded and split per window), about one wave of single-CTA SMs in all
+  // about one wave of single-CTA SMs
   int nsm = 148;
   {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   }
-  for (int q = 0; q < job.nunit; ++q) {
-    TcUnit& u = job.u[q];
-    long long nc = (long long)nsm * (128 + u.nn) / wsum;
-    if (nc < 1) nc = 1;
-    if (nc > job.kb_total) nc = job.kb_total;
-    u.cta0 = (short)job.ncta;
-    u.nchunk = (short)nc;
-    job.ncta += (int)nc;
-  }
-  float* part = (float*)scratch(c, hfb_ctx_s::S_GRAM, sizeof(float) * (size_t)job.ncta * 128 * kTcMaxNp);
+  job.kchunks = nsm / job.nunit;
+  if (job.kchunks < 1) job.kchunks = 1;
+  if (job.kchunks > job.kb_total) job.kchunks = job.kb_total;
+  const int ncta = job.nunit * job.kchunks;
+  float* part = (float*)scratch(c, hfb_ctx_s::S_GRAM, sizeof(float) * (size_t)ncta * 128 * kTcMaxNp);
   if (!part) return HFB_ERR_ALLOC;
-  const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)nnmax * 128);
+  int npmax = 16;
+  for (int b = 0; b < nblk; ++b) npmax = job.np[b] > npmax ? job.np[b] : npmax;
+  const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)npmax * 128);
   cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  gram_tc_kernel<<<job.ncta, kTcThreads, smem, st>>>(job, (const float*)psi, (const float*)hampsi,
-                                                     (const float*)hmfpsi, part, c->dev_status);
+  gram_tc_kernel<<<ncta, kTcThreads, smem, st>>>(job, (const float*)psi, (const float*)hampsi,
+                                                 (const float*)hmfpsi, part, c->dev_status);
   HFB_CHECK_LAUNCH();
   TcOut ot;
   for (int q = 0; q < 8; ++q) ot.p[q] = outs_host[q];
