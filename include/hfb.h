@@ -208,6 +208,15 @@ int hfb_gram(hfb_ctx_t ctx, int prec, int s0, int ns, int mask, const void* psi,
  * int[nb]) receives the number of Jacobi sweeps each matrix took. */
 int hfb_eigh(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w, double* v,
              int* sweeps, void* stream);
+/* Hermitian eigensolver for matrices that are close to diagonal (the lambda
+ * matrix of a gradient step in the basis of the previous eigenvectors):
+ * iterative refinement from X = I with the (near-)degenerate clusters
+ * diagonalised exactly, cyclic Jacobi when the refinement does not apply.
+ * Same contract as hfb_eigh (lower triangle read, w ascending, columns of v
+ * the eigenvectors); lda <= 256.  hfb_diagstep uses it for lambda, the
+ * eigh of static.py:300-310 / 397-407. */
+int hfb_eigh_near_diagonal(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w,
+                           double* v, void* stream);
 
 /* ---- pairs.py ---------------------------------------------------------- */
 typedef struct hfb_pair_args {

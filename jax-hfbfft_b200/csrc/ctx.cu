@@ -84,6 +84,8 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
   {
     const char* e = getenv("HFB_NO_TCGEN05");
     c->use_tcgen05 = (e && e[0] == '1') ? 0 : 1;
+    const char* j = getenv("HFB_LAMBDA_JACOBI");
+    c->lambda_refine = (j && j[0] == '1') ? 0 : 1;
   }
   const size_t nn = (size_t)nx * nx;
   for (int a = 0; a < 3; ++a) {

@@ -18,9 +18,11 @@ struct hfb_ctx_s {
   cudaStream_t side;     // secondary stream for independent work inside a call
   int use_tcgen05;       // single-precision contractions on the tensor cores (default 1;
                          // HFB_NO_TCGEN05=1 in the environment at creation selects CUDA cores)
+  int lambda_refine;     // FP64 diagstep diagonalises lambda by eigen refinement (default 1;
+                         // HFB_LAMBDA_JACOBI=1 at creation selects the Jacobi solver)
   cudaEvent_t ev_fork, ev_join;
   // scratch arena: fixed slots, grown on demand (never shrunk)
-  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_NSLOT };
+  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_NSLOT };
   void* slot[S_NSLOT];
   size_t slot_bytes[S_NSLOT];
 };

@@ -82,6 +82,7 @@ _PROTOS = {
     "hfb_diagstep": [vp, C.c_int, C.POINTER(DiagArgs), vp],
     "hfb_gram": [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, vp, vp],
     "hfb_eigh": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
+    "hfb_eigh_near_diagonal": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp],
     "hfb_pair": [vp, C.POINTER(PairArgs), vp],
     "hfb_energies": [vp, C.POINTER(HfbForce), C.c_int, C.c_double] + [vp] * 6 + [vp, vp, vp],
     "hfb_sum_energy": [vp, C.c_int] + [vp] * 6 + [vp, vp],

@@ -3,7 +3,7 @@ profiler captures).
 
     python -m hfb.microbench hpsi    [--case Pb208] [--states S] [--prec f32|f64] [--reps R]
     python -m hfb.microbench gram    [--case Pb208] [--prec f32|f64] [--reps R]
-    python -m hfb.microbench iterate [--case Pb208] [--prec f32|f64] [--reps R]
+    python -m hfb.microbench iterate [--case Pb208] [--prec f32|f64] [--reps R] [--skip N]
 
 Every mode builds the workload's oscillator start and its mean field
 (``static.prepare``), runs the operation ``--warmup`` times and then ``--reps``
@@ -96,8 +96,10 @@ def run_iterate(args, dtype):
         it[0] += 1
         static.iterate(it[0], **S)
 
+    for _ in range(args.skip):
+        once()
     t = _time(once, args.warmup, args.reps)
-    return dict(op="iterate", seconds=t, energy=st["energies"].ehf)
+    return dict(op="iterate", seconds=t, energy=st["energies"].ehf, first_timed_iteration=args.skip + args.warmup + 1)
 
 
 def main(argv=None):
@@ -108,6 +110,7 @@ def main(argv=None):
     ap.add_argument("--states", type=int, default=0)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--skip", type=int, default=0, help="iterate: untimed iterations before the warm-up")
     args = ap.parse_args(argv)
     dtype = torch.complex64 if args.prec == "f32" else torch.complex128
     fn = {"hpsi": run_hpsi, "gram": run_gram, "iterate": run_iterate}[args.op]

@@ -400,3 +400,44 @@ def test_diagstep_single_precision_matches_double():
     e32 = l32.sp_energy.cpu().numpy()
     e64 = l64.sp_energy.cpu().numpy()
     assert np.max(np.abs(np.sort(e32) - np.sort(e64))) < 2e-2
+
+
+def _near_diag_hermitian(n, seed, scale, kramers=True):
+    """Hermitian test matrix close to diagonal: spread diagonal with exactly
+    degenerate pairs (as time reversal gives), plus a random Hermitian
+    coupling of size ``scale``."""
+    rng = np.random.default_rng(seed)
+    d = np.sort(rng.uniform(-60.0, 40.0, (n + 1) // 2))
+    diag = np.repeat(d, 2)[:n] if kramers else np.sort(rng.uniform(-60.0, 40.0, n))
+    h = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    h = scale * (h + h.conj().T) / 2
+    return np.diag(diag) + h
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,scale,kramers", [(140, 1e-3, True), (96, 1e-2, True), (40, 1e-4, False),
+                                             (140, 5.0, True)])
+def test_eigh_near_diagonal(n, scale, kramers):
+    """hfb_eigh_near_diagonal (iterative refinement + exact cluster solves,
+    Jacobi when it does not apply; the last case is far from diagonal)
+    against numpy: eigenvalues, residual ||A V - V W|| and orthonormality."""
+    import hfb
+    from hfb._lib import call, ptr, stream_ptr
+    p = hfb.params.init_params()
+    g = hfb.grids.init_grids(p, nx=8, ny=8, nz=8, dx=1.0, dy=1.0, dz=1.0)
+    nb = 3
+    a = np.stack([_near_diag_hermitian(n, 5 + k, scale, kramers) for k in range(nb)])
+    # the solver reads the lower triangle only
+    a_in = np.tril(a) + np.triu(np.full_like(a, 7.0 + 3.0j), 1)
+    ta = T(a_in)
+    w = torch.zeros((nb, n), dtype=torch.float64, device="cuda")
+    v = torch.zeros((nb, n, n), dtype=torch.complex128, device="cuda")
+    call("hfb_eigh_near_diagonal", g.ctx.handle, nb, n, n, ptr(ta), ptr(w), ptr(v), stream_ptr())
+    torch.cuda.synchronize()
+    wv, vv = w.cpu().numpy(), v.cpu().numpy()
+    for k in range(nb):
+        ref = np.linalg.eigvalsh(a[k])
+        amax = np.abs(ref).max()
+        assert np.max(np.abs(wv[k] - ref)) < 1e-12 * amax * n
+        assert np.max(np.abs(a[k] @ vv[k] - vv[k] * wv[k][None, :])) < 1e-11 * amax
+        assert np.max(np.abs(vv[k].conj().T @ vv[k] - np.eye(n))) < 1e-12
