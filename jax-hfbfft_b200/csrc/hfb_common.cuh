@@ -201,9 +201,9 @@ template <class R, int N_, int P_> struct Pencil {
   __device__ __forceinline__ static int freq(int q, int t, int k1) { return q + P * t + M * k1; }
   __device__ __forceinline__ static bool valid(int q, int t) { return q + P * t < M; }
 
+  // e = p k2 with p < P and k2 < M at every call, so e <= (P - 1)(M - 1) < N
   template <int SIGN>
   __device__ __forceinline__ static Z tw_mul(Z x, const Z* tw, int e) {
-    e %= N;
     Z w = tw[e];
     if (SIGN > 0) w.y = -w.y;
     return cmul(x, w);

@@ -25,42 +25,80 @@ struct DerivJobs {
   DerivJob j[kMaxJobs];
 };
 
-__global__ void deriv_jobs_kernel(DerivJobs jobs, int n, const double* d1x, const double* d1y, const double* d1z,
-                                  const double* d2x, const double* d2y, const double* d2z) {
+// Term t of every job as dense line transforms on shared-memory tiles: a
+// block stages one plane of the input (the x-plane for y and z lines, the
+// y-plane for x lines: n lines of n points) and the n x n derivative matrix,
+// and each thread forms 4 x 4 outputs (4 lines x 4 derivative points).
+// Term 0 writes coef * D f, later terms add to it (fixed order).
+constexpr int kDerivMaxN = 48;
+
+__global__ void __launch_bounds__(144)
+deriv_pass_kernel(DerivJobs jobs, int t, int n, const double* d1x, const double* d1y, const double* d1z,
+                  const double* d2x, const double* d2y, const double* d2z) {
+  __shared__ double F[kDerivMaxN][kDerivMaxN + 1];   // [line][point along the axis]
+  __shared__ double Dm[kDerivMaxN][kDerivMaxN + 1];  // [output point][input point]
   const DerivJob& jb = jobs.j[blockIdx.y];
-  const size_t n3 = (size_t)n * n * n;
-  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= n3) return;
-  const int x = (int)(i / ((size_t)n * n)), y = (int)((i / n) % n), z = (int)(i % n);
-  double acc = 0.0;
-  for (int t = 0; t < jb.nterm; ++t) {
-    const int ax = jb.axis[t];
-    const double* D = jb.der[t] == 1 ? (ax == 0 ? d1x : ax == 1 ? d1y : d1z) : (ax == 0 ? d2x : ax == 1 ? d2y : d2z);
-    const double* f = jb.in[t];
-    double s = 0.0;
-    if (ax == 0) {
-      const double* row = D + (size_t)x * n;
-      for (int l = 0; l < n; ++l) s += row[l] * f[(size_t)l * n * n + (size_t)y * n + z];
-    } else if (ax == 1) {
-      const double* row = D + (size_t)y * n;
-      for (int l = 0; l < n; ++l) s += row[l] * f[(size_t)x * n * n + (size_t)l * n + z];
-    } else {
-      const double* row = D + (size_t)z * n;
-      const double* fl = f + (size_t)x * n * n + (size_t)y * n;
-      for (int l = 0; l < n; ++l) s += row[l] * fl[l];
-    }
-    acc += jb.coef[t] * s;
+  if (t >= jb.nterm) return;
+  const int ax = jb.axis[t];
+  const double* D = jb.der[t] == 1 ? (ax == 0 ? d1x : ax == 1 ? d1y : d1z) : (ax == 0 ? d2x : ax == 1 ? d2y : d2z);
+  const double* f = jb.in[t];
+  const double coef = jb.coef[t];
+  const size_t n2 = (size_t)n * n;
+  const int tile = blockIdx.x;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, q = e % n;   // q runs over the contiguous index
+    Dm[r][q] = D[e];
+    if (ax == 2) F[r][q] = f[tile * n2 + (size_t)r * n + q];          // line y = r, point z = q
+    else if (ax == 1) F[q][r] = f[tile * n2 + (size_t)r * n + q];     // line z = q, point y = r
+    else F[q][r] = f[(size_t)r * n2 + (size_t)tile * n + q];          // line z = q, point x = r
   }
-  jb.out[i] = acc;
+  __syncthreads();
+  const int g = n / 4, nthr = g * g;
+  if ((int)threadIdx.x >= nthr) return;
+  // consecutive threads run along the output's contiguous index
+  const int tfast = threadIdx.x % g, tslow = threadIdx.x / g;
+  const int tl = ax == 2 ? tslow : tfast, tk = ax == 2 ? tfast : tslow;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int l = 0; l < n; ++l) {
+    double fv[4], dv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) fv[i] = F[tl + g * i][l];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dv[j] = Dm[tk + g * j][l];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] += dv[j] * fv[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int line = tl + g * i, k = tk + g * j;
+      size_t o;
+      if (ax == 2) o = tile * n2 + (size_t)line * n + k;
+      else if (ax == 1) o = tile * n2 + (size_t)k * n + line;
+      else o = (size_t)k * n2 + (size_t)tile * n + line;
+      const double v = coef * acc[i][j];
+      jb.out[o] = t == 0 ? v : jb.out[o] + v;
+    }
 }
 
 static int run_jobs(hfb_ctx_s* c, DerivJobs& jobs, int nj, cudaStream_t st) {
   if (nj <= 0) return HFB_OK;
-  const size_t n3 = (size_t)c->n * c->n * c->n;
-  dim3 grid((unsigned)((n3 + 255) / 256), nj);
-  deriv_jobs_kernel<<<grid, 256, 0, st>>>(jobs, c->n, c->der1[0], c->der1[1], c->der1[2], c->der2[0], c->der2[1],
-                                          c->der2[2]);
-  HFB_CHECK_LAUNCH();
+  if (c->n > kDerivMaxN || c->n % 4 != 0) return HFB_ERR_UNSUPPORTED_GRID;
+  int tmax = 0;
+  for (int q = 0; q < nj; ++q) tmax = jobs.j[q].nterm > tmax ? jobs.j[q].nterm : tmax;
+  dim3 grid((unsigned)c->n, nj);
+  for (int t = 0; t < tmax; ++t) {
+    deriv_pass_kernel<<<grid, 144, 0, st>>>(jobs, t, c->n, c->der1[0], c->der1[1], c->der1[2], c->der2[0],
+                                            c->der2[1], c->der2[2]);
+    HFB_CHECK_LAUNCH();
+  }
   return HFB_OK;
 }
 
