@@ -87,6 +87,22 @@ __global__ void energy_final_kernel(hfb_force f, int tcoul, double A, double wxy
     s[threadIdx.x] = wxyz * v;
   }
   __syncthreads();
+  // energies.py:157-167 (diagnostic; indexes current[iq, comp, x, c, s] with
+  // y = c, z = s): the 2 x 3 x n x 3 terms spread over the warp
+  const size_t n3 = (size_t)n * n * n;
+  double cj0 = 0.0, cj1 = 0.0;
+  for (int e = threadIdx.x; e < 2 * 3 * n * 3; e += blockDim.x) {
+    const int c = e % 3, x = (e / 3) % n, comp = (e / (3 * n)) % 3, iq = e / (9 * n);
+    const double* base = cur + ((size_t)iq * 3 + comp) * n3 + (size_t)x * n * n + (size_t)c * n;
+    const double a0 = base[0], a1 = base[1];
+    cj0 += (a0 + a1) * (a0 + a1);
+    cj1 += (-a0 + a1) * (-a0 + a1);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cj0 += __shfl_xor_sync(0xffffffffu, cj0, o);
+    cj1 += __shfl_xor_sync(0xffffffffu, cj1, o);
+  }
   if (threadIdx.x != 0) return;
   const double ep = epair[0] + epair[1];
   const double ehf3 = s[I_EHF3];
@@ -95,18 +111,6 @@ __global__ void energy_final_kernel(hfb_force f, int tcoul, double A, double wxy
   const double ezpe = f.zpe == 1 ? 17.3 / pow(A, 0.2) : 0.0;
   const double ehfc = tcoul ? s[I_EHFC] : 0.0, ecorc = tcoul ? s[I_ECORC] : 0.0;
   const double ehfint = s[I_EHFT] + s[I_EHF0] + s[I_EHF1] + s[I_EHF2] + ehf3 + ehfls + ehfc - ep - ezpe;
-  // energies.py:157-167 (diagnostic; indexes current[iq, comp, x, c, s] with y = c, z = s)
-  const size_t n3 = (size_t)n * n * n;
-  double cj0 = 0.0, cj1 = 0.0;
-  for (int iq = 0; iq < 2; ++iq)
-    for (int comp = 0; comp < 3; ++comp)
-      for (int x = 0; x < n; ++x)
-        for (int c = 0; c < 3; ++c) {
-          const double* base = cur + ((size_t)iq * 3 + comp) * n3 + (size_t)x * n * n + (size_t)c * n;
-          const double a0 = base[0], a1 = base[1];
-          cj0 += (a0 + a1) * (a0 + a1);
-          cj1 += (-a0 + a1) * (-a0 + a1);
-        }
   out[HFB_E_EHFT] = s[I_EHFT];
   out[HFB_E_EHF0] = s[I_EHF0];
   out[HFB_E_EHF1] = s[I_EHF1];

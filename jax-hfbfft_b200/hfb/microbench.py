@@ -96,10 +96,16 @@ def run_iterate(args, dtype):
         it[0] += 1
         static.iterate(it[0], **S)
 
+    from ._lib import launch_count
+    l0 = launch_count()
     for _ in range(args.skip):
         once()
+    l1 = launch_count()
     t = _time(once, args.warmup, args.reps)
-    return dict(op="iterate", seconds=t, energy=st["energies"].ehf, first_timed_iteration=args.skip + args.warmup + 1)
+    l2 = launch_count()
+    return dict(op="iterate", seconds=t, energy=st["energies"].ehf, first_timed_iteration=args.skip + args.warmup + 1,
+                launches_before_timed=l1 + (l2 - l1) * args.warmup // (args.warmup + args.reps),
+                launches_setup=l0, launches_per_iteration=(l2 - l1) / (args.warmup + args.reps))
 
 
 def main(argv=None):
