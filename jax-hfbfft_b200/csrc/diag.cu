@@ -1376,9 +1376,18 @@ rotate_f32_kernel(int ns, size_t K, const float2* __restrict__ psi, const double
   }
 }
 
+int rotate_tc_launch(hfb_ctx_s* c, int ns, const void* psi, const double2* U, const double2* L, int ld, void* out1,
+                     void* out2, cudaStream_t st);   // rotate_tc.cu
+
 int rotate_launch(hfb_ctx_s* c, int prec, int s0, int ns, const void* psi, const double2* U, const double2* L, int ld,
                   void* out1, void* out2, cudaStream_t st) {
   if (ns <= 0) return HFB_OK;
+  if (prec != HFB_F64 && c->use_tcgen05) {
+    const size_t Kc = (size_t)2 * c->n * c->n * c->n, offc = (size_t)s0 * Kc;
+    const int r = rotate_tc_launch(c, ns, (const float2*)psi + offc, U, L, ld, (float2*)out1 + offc,
+                                   (float2*)out2 + offc, st);
+    if (r != HFB_ERR_UNSUPPORTED_GRID) return r;
+  }
   const size_t K = (size_t)2 * c->n * c->n * c->n;
   const int njt = (2 * ns + 63) / 64;
   const size_t nkt = (K + 63) / 64;
