@@ -70,6 +70,9 @@ int hfb_ctx_destroy(hfb_ctx_t ctx);
 const char* hfb_status_string(int status);
 /* Number of kernels this library has launched in the process. */
 unsigned long long hfb_launch_count(void);
+/* The CUDA error behind the last HFB_ERR_CUDA returned to this host thread
+ * (code in *code when code is not NULL; 0 and "no CUDA error" if none). */
+const char* hfb_last_cuda_error(int* code);
 /* Latched device-side status (synchronises the stream), then clears it. */
 int hfb_device_status(hfb_ctx_t ctx, void* stream, int* status_out);
 

@@ -11,6 +11,8 @@ namespace hfb {
 
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+static thread_local int t_last_cuda_error = 0;
+void note_cuda_error(int e) { t_last_cuda_error = e; }
 
 int coulomb_init(hfb_ctx_s* c);  // skyrme.cu
 
@@ -146,6 +148,12 @@ extern "C" int hfb_ctx_destroy(hfb_ctx_t c) {
 }
 
 extern "C" unsigned long long hfb_launch_count(void) { return hfb::g_launches.load(); }
+
+extern "C" const char* hfb_last_cuda_error(int* code) {
+  const int e = hfb::t_last_cuda_error;
+  if (code) *code = e;
+  return e ? cudaGetErrorString((cudaError_t)e) : "no CUDA error";
+}
 
 extern "C" const char* hfb_status_string(int s) {
   switch (s) {

@@ -547,13 +547,13 @@ int eigh_batch(hfb_ctx_s* c, EighBatch eb, cudaStream_t st) {
   if (!buf) return HFB_ERR_ALLOC;
   JacRot* rot = (JacRot*)buf;
   int* nr = (int*)(buf + sizeof(JacRot) * rot_stride * eb.nb);
-  cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  allow_max_dynamic_smem(jacobi_kernel);
   jacobi_kernel<<<eb.nb, kJacThreads, smem, st>>>(eb, rot, nr, c->dev_status, rot_stride);
   HFB_CHECK_LAUNCH();
   eb.stage_half = half;
   const size_t smem2 =
       sizeof(JacRot) * 2 * kVecChunk * half + sizeof(double2) * kVecRows * mmax + sizeof(int) * mmax;
-  cudaFuncSetAttribute(jacobi_vectors_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+  allow_max_dynamic_smem(jacobi_vectors_kernel);
   jacobi_vectors_kernel<<<eb.vblk0[eb.nb], 256, smem2, st>>>(eb, rot, nr, rot_stride);
   HFB_CHECK_LAUNCH();
   sort_values_kernel<<<eb.nb, 256, sizeof(double) * nmax, st>>>(eb);

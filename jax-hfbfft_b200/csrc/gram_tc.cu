@@ -336,7 +336,7 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
   int npmax = 16;
   for (int b = 0; b < nblk; ++b) npmax = job.np[b] > npmax ? job.np[b] : npmax;
   const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)npmax * 128);
-  cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  allow_max_dynamic_smem(gram_tc_kernel);
   gram_tc_kernel<<<ncta, kTcThreads, smem, st>>>(job, (const float*)psi, (const float*)hampsi,
                                                  (const float*)hmfpsi, part, c->dev_status);
   HFB_CHECK_LAUNCH();

@@ -250,13 +250,9 @@ int precond_launch_t(hfb_ctx_s* c, int ns, int nneut, const void* src, const voi
   using G = PlaneGeo<R, N>;
   using Z = cplx<R>;
   if (ns <= 0) return HFB_OK;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(precond_a_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
-    cudaFuncSetAttribute(precond_b_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
-    cudaFuncSetAttribute(precond_c_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
-    attr = true;
-  }
+  allow_max_dynamic_smem(precond_a_kernel<R, N>);
+  allow_max_dynamic_smem(precond_b_kernel<R, N>);
+  allow_max_dynamic_smem(precond_c_kernel<R, N>);
   dim3 grid(N, ns);
   precond_a_kernel<R, N><<<grid, G::THREADS, G::SMEM, st>>>((const Z*)src, (const Z*)lag, use_lag, (const Z*)psi,
                                                             coef, (Z*)tmp, fluct);

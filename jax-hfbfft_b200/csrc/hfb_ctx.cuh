@@ -35,13 +35,39 @@ void* scratch(hfb_ctx_s* c, int s, size_t bytes);
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // Counts every kernel launch of the library (reported by hfb_launch_count).
+// Allow a kernel all the dynamic shared memory the device opts in to (the
+// opt-in maximum less the kernel's static shared memory).  Every call sets
+// the same value for a kernel, so host threads launching it concurrently
+// with different shared-memory sizes never lower the limit under one
+// another's launches.
+template <class F>
+inline void allow_max_dynamic_smem(F* fn) {
+  static const int optin = [] {
+    int d = 0, v = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, d);
+    return v;
+  }();
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes) !=
+      cudaSuccess)
+    cudaGetLastError();
+}
+void note_cuda_error(int e);   // the CUDA error behind the last HFB_ERR_CUDA of this host thread
 void count_launch();
 
 #define HFB_CHECK_LAUNCH()                                            \
   do {                                                                \
     hfb::count_launch();                                              \
     cudaError_t e_ = cudaGetLastError();                              \
-    if (e_ != cudaSuccess) return HFB_ERR_CUDA;                       \
+    if (e_ != cudaSuccess) {                                          \
+      hfb::note_cuda_error((int)e_);                                  \
+      return HFB_ERR_CUDA;                                            \
+    }                                                                 \
   } while (0)
 
 // Supported cubic grid sizes; ``fn`` is a generic lambda taking

@@ -313,12 +313,8 @@ int hpsi_launch_t(hfb_ctx_s* c, const void* pot, int s0, int ns, int nneut, cons
     ks[a] = kf[a] / N;
     nq[a] = (kPi / c->d[a]) * (kPi / c->d[a]) / N;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(hpsi_xplane_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
-    cudaFuncSetAttribute(hpsi_yplane_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
-    attr_set = true;
-  }
+  allow_max_dynamic_smem(hpsi_xplane_kernel<R, N>);
+  allow_max_dynamic_smem(hpsi_yplane_kernel<R, N>);
   dim3 grid(N, ns);
   hpsi_xplane_kernel<R, N><<<grid, G::THREADS, G::SMEM, st>>>((const R*)pot, (const Z*)psi, (Z*)acc, s0, nneut, ks[1],
                                                              ks[2], nq[1], nq[2]);

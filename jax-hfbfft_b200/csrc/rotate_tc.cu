@@ -315,7 +315,7 @@ int rotate_tc_launch(hfb_ctx_s* c, int ns, const void* psi, const double2* U, co
   }
   const int grid = job.ntask < nsm ? job.ntask : nsm;
   const size_t smem = 1024 + (size_t)kRtStages * kRtStage;
-  cudaFuncSetAttribute(rotate_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  allow_max_dynamic_smem(rotate_tc_kernel);
   rotate_tc_kernel<<<grid, kRtThreads, smem, st>>>(job, (const float*)psiT, bt, (float2*)out1, (float2*)out2,
                                                    c->dev_status);
   HFB_CHECK_LAUNCH();

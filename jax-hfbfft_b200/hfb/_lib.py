@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libhfb.so")
 
 HFB_OK = 0
+HFB_ERR_CUDA = 3
 HFB_F64 = 0
 HFB_F32 = 1
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported grid", 3: "CUDA error",
@@ -89,7 +90,7 @@ _PROTOS = {
     "hfb_energy_grad": [vp, C.POINTER(HfbForce)] + [vp] * 5 + [vp, vp],
     "hfb_rms": [vp, vp, vp, vp],
 }
-SYMBOLS = tuple(_PROTOS) + ("hfb_status_string", "hfb_launch_count")
+SYMBOLS = tuple(_PROTOS) + ("hfb_status_string", "hfb_launch_count", "hfb_last_cuda_error")
 
 _lib = None
 
@@ -110,13 +111,15 @@ def load():
     lib.hfb_status_string.restype = C.c_char_p
     lib.hfb_launch_count.argtypes = []
     lib.hfb_launch_count.restype = C.c_ulonglong
+    lib.hfb_last_cuda_error.argtypes = [C.POINTER(C.c_int)]
+    lib.hfb_last_cuda_error.restype = C.c_char_p
     _lib = lib
     return lib
 
 
 class HfbError(RuntimeError):
-    def __init__(self, fn, code):
-        super().__init__(f"{fn}: {STATUS.get(code, 'unknown status')} (status {code})")
+    def __init__(self, fn, code, detail=""):
+        super().__init__(f"{fn}: {STATUS.get(code, 'unknown status')} (status {code}){detail}")
         self.code = code
 
 
@@ -124,7 +127,12 @@ def call(name, *args):
     """Call a library function and raise HfbError on a non-zero status."""
     r = getattr(load(), name)(*args)
     if r != HFB_OK:
-        raise HfbError(name, r)
+        detail = ""
+        if r == HFB_ERR_CUDA:
+            e = C.c_int(0)
+            msg = load().hfb_last_cuda_error(C.byref(e)).decode()
+            detail = f": cudaError {e.value} ({msg})"
+        raise HfbError(name, r, detail)
     return r
 
 
