@@ -376,7 +376,17 @@ def main():
     peak, peak_kind = _peaks()
     achieved = b_h / t_h / 1e9
     from hfb.output import rms_radii
+    import numpy as np
     _, rms, _ = rms_radii(rm["state"]["densities"], rm["state"]["grids"])
+    _, rms64, _ = rms_radii(r64["state"]["densities"], r64["state"]["grids"])
+
+    def _spe(st):
+        lv = st["levels"]
+        e = lv.sp_energy.detach().cpu().numpy()
+        n0 = lv.npsi[0]
+        return np.concatenate([np.sort(e[:n0]), np.sort(e[n0:])])
+
+    d_spe = float(np.max(np.abs(_spe(rm["state"]) - _spe(r64["state"]))))
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=im + 1 if im is not None else rm["iters"],
         warmup=max(args.warmup, 3), ms_per_step=(value / (im + 1) * 1e3) if value else None, higher_is_better=False,
@@ -390,6 +400,7 @@ def main():
                     mixed_iterations=(im + 1) if im is not None else None, mixed_switch_iteration=rm["switch"],
                     e_ref_mev=e_ref, e_mixed_final_mev=rm["E"][-1],
                     de_final_kev=abs(rm["E"][-1] - e_ref) * 1e3, rms_proton_fm=rms[1],
+                    d_rms_proton_fm_vs_fp64=abs(rms[1] - rms64[1]), d_sp_energy_max_mev_vs_fp64=d_spe,
                     fp64_ms_per_iteration=(r64["t"][-1] / r64["iters"] * 1e3)),
         roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                       traffic=HPSI_NCU_DRAM_BYTES, kernel="hpsi (hpsi_xplane + hpsi_yplane), FP32, 236 states",

@@ -938,7 +938,7 @@ __global__ void ref_assemble_kernel(int ld, Pair2 nper, RefWork w, double* W, si
 // (static.py:470-480) whenever no eigenvalue of S falls below its floor
 // max(1e-12, eps max(w) n); S is then positive definite with condition far
 // from that floor.  Steps after convergence are retired on the device.
-constexpr int kNSMaxIt = 24;
+constexpr int kNSMaxIt = 16;   // S is close to I after a gradient step: 4-6 steps in practice
 
 // c_b and the start Y = S / c, Z = I; gate = large.
 __global__ void ns_init_kernel(int ld, Pair2 nper, const double2* S, size_t sS, double2* Y, double2* Z, size_t sm,
