@@ -386,12 +386,20 @@ def main():
     _, rms64, _ = rms_radii(r64["state"]["densities"], r64["state"]["grids"])
 
     def _spe(st):
+        # single-particle energies and occupations, each isospin sorted by energy
         lv = st["levels"]
         e = lv.sp_energy.detach().cpu().numpy()
+        w = lv.wocc.detach().cpu().numpy()
         n0 = lv.npsi[0]
-        return np.concatenate([np.sort(e[:n0]), np.sort(e[n0:])])
+        o0, o1 = np.argsort(e[:n0], kind="stable"), n0 + np.argsort(e[n0:], kind="stable")
+        idx = np.concatenate([o0, o1])
+        return e[idx], w[idx]
 
-    d_spe = float(np.max(np.abs(_spe(rm["state"]) - _spe(r64["state"]))))
+    e_m, _ = _spe(rm["state"])
+    e_64, w_64 = _spe(r64["state"])
+    d_spe = float(np.max(np.abs(e_m - e_64)))
+    occ = w_64 > 1e-2
+    d_spe_occ = float(np.max(np.abs(e_m - e_64)[occ])) if occ.any() else None
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=im + 1 if im is not None else rm["iters"],
         warmup=max(args.warmup, 3), ms_per_step=(value / (im + 1) * 1e3) if value else None, higher_is_better=False,
@@ -406,6 +414,7 @@ def main():
                     e_ref_mev=e_ref, e_mixed_final_mev=rm["E"][-1],
                     de_final_kev=abs(rm["E"][-1] - e_ref) * 1e3, rms_proton_fm=rms[1],
                     d_rms_proton_fm_vs_fp64=abs(rms[1] - rms64[1]), d_sp_energy_max_mev_vs_fp64=d_spe,
+                    d_sp_energy_occupied_max_mev_vs_fp64=d_spe_occ,
                     fp64_ms_per_iteration=(r64["t"][-1] / r64["iters"] * 1e3)),
         roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                       traffic=HPSI_NCU_DRAM_BYTES, kernel="hpsi (hpsi_xplane + hpsi_yplane), FP32, 236 states",
