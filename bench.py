@@ -174,7 +174,7 @@ def fp64_run(case_name, maxiter):
     return dict(E=E, t=t, e_ref=E[-1] + rem, iters=len(E), state=st)
 
 
-def mixed_e2e_run(case_name, maxiter):
+def mixed_e2e_run(case_name, maxiter, switch_mev=5e-4):
     """Mixed run through hfb.static.statichf_mixed.  The initial states are
     copied from pinned host memory inside the timed region; E_bind, the
     densities and the single-particle energies are read back at the end."""
@@ -203,7 +203,8 @@ def mixed_e2e_run(case_name, maxiter):
     e_h2d0.record()
     st["levels"].psi.copy_(host_psi, non_blocking=True)
     e_h2d1.record()
-    hist, sw = static.statichf_mixed(st, maxiter=maxiter, stop_mev=STOP_MEV, on_iteration=on_it)
+    hist, sw = static.statichf_mixed(st, maxiter=maxiter, switch_mev=switch_mev, stop_mev=STOP_MEV,
+                                     on_iteration=on_it)
     e_d2h0.record()
     out_rho = st["densities"].rho.to("cpu", non_blocking=True)
     out_spe = st["levels"].sp_energy.to("cpu", non_blocking=True)
@@ -332,6 +333,8 @@ def main():
     ap.add_argument("--workload", default="Pb208")
     ap.add_argument("--tol-kev", type=float, default=1.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--switch-mev", type=float, default=5e-4,
+                    help="mixed run: estimated remaining change (MeV) at which FP32 hands over to FP64")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -364,7 +367,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        rm = mixed_e2e_run(args.workload, maxiter)
+        rm = mixed_e2e_run(args.workload, maxiter, args.switch_mev)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
