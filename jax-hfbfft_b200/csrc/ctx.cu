@@ -15,6 +15,7 @@ static thread_local int t_last_cuda_error = 0;
 void note_cuda_error(int e) { t_last_cuda_error = e; }
 
 int coulomb_init(hfb_ctx_s* c);  // skyrme.cu
+int hpsi_tc_prepare(hfb_ctx_s* c);  // hpsi_tc.cu
 
 void* scratch(hfb_ctx_s* c, int s, size_t bytes) {
   if (s < 0 || s >= hfb_ctx_s::S_NSLOT) return nullptr;
@@ -118,6 +119,7 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     return HFB_ERR_ALLOC;
   }
   int r = coulomb_init(c);
+  if (r == HFB_OK) r = hpsi_tc_prepare(c);
   if (r == HFB_OK && cudaDeviceSynchronize() != cudaSuccess) r = HFB_ERR_CUDA;
   if (r != HFB_OK) {
     hfb_ctx_destroy(c);
@@ -135,6 +137,7 @@ extern "C" int hfb_ctx_destroy(hfb_ctx_t c) {
     if (c->der2[a]) cudaFree(c->der2[a]);
   }
   if (c->coul_q) cudaFree(c->coul_q);
+  if (c->hpsi_b) cudaFree(c->hpsi_b);
   if (c->dev_status) cudaFree(c->dev_status);
   if (c->side) {
     cudaStreamDestroy(c->side);

@@ -384,11 +384,12 @@ extern "C" int hfb_grstep(hfb_ctx_t ctx, int prec, const hfb_grstep_args* a, voi
   const int ns = a->nst, n = ctx->n;
   if (ns <= 0) return HFB_OK;
   const size_t n3 = (size_t)n * n * n;
-  double* part = (double*)scratch(ctx, hfb_ctx_s::S_PART, sizeof(double) * (size_t)ns * n * 2 * 2);
+  const int nov = hpsi_ovl_parts(ctx, prec);
+  double* part = (double*)scratch(ctx, hfb_ctx_s::S_PART, sizeof(double) * (size_t)ns * (nov + n) * 2);
   double* vec = (double*)scratch(ctx, hfb_ctx_s::S_SMALL, sizeof(double) * ((size_t)ns * 6 + 8));
   if (!part || !vec) return HFB_ERR_ALLOC;
   double* ovl = part;
-  double* fl = part + (size_t)ns * n * 2;
+  double* fl = part + (size_t)ns * nov * 2;
   double *wt = vec, *wu = vec + ns, *lw = vec + 2 * ns, *lu = vec + 3 * ns, *spe_new = vec + 4 * ns,
          *hexp = vec + 5 * ns, *vmax = vec + 6 * ns;
   grstep_weights_kernel<<<(ns + 127) / 128, 128, 0, st>>>(ns, a->tbcs, a->wocc, a->wguv, a->pairwg, a->wstates, wt,
@@ -400,9 +401,9 @@ extern "C" int hfb_grstep(hfb_ctx_t ctx, int prec, const hfb_grstep_args* a, voi
   int r = hpsi_launch(ctx, prec, a->pot, 0, ns, a->nneut, a->psi, wt, wu, a->hampsi, a->hmfpsi, a->hampsi, nullptr,
                       ovl, st);
   if (r) return r;
-  state_reduce_kernel<<<(ns + 127) / 128, 128, 0, st>>>(ns, n, ovl, 0, a->wxyz, spe_new);
+  state_reduce_kernel<<<(ns + 127) / 128, 128, 0, st>>>(ns, nov, ovl, 0, a->wxyz, spe_new);
   HFB_CHECK_LAUNCH();
-  state_reduce_kernel<<<(ns + 127) / 128, 128, 0, st>>>(ns, n, ovl, 1, a->wxyz, hexp);
+  state_reduce_kernel<<<(ns + 127) / 128, 128, 0, st>>>(ns, nov, ovl, 1, a->wxyz, hexp);
   HFB_CHECK_LAUNCH();
   // 2) damped step
   if (a->e0dmp > 0.0) {

@@ -21,8 +21,9 @@ struct hfb_ctx_s {
   int lambda_refine;     // FP64 diagstep diagonalises lambda by eigen refinement (default 1;
                          // HFB_LAMBDA_JACOBI=1 at creation selects the Jacobi solver)
   cudaEvent_t ev_fork, ev_join;
+  unsigned char* hpsi_b; // single-precision hpsi: derivative matrices in the tensor-core tile layout
   // scratch arena: fixed slots, grown on demand (never shrunk)
-  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_NSLOT };
+  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_HPT, S_NSLOT };
   void* slot[S_NSLOT];
   size_t slot_bytes[S_NSLOT];
 };

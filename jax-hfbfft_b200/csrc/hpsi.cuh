@@ -5,11 +5,24 @@
 namespace hfb {
 
 // hpsi on states [s0, s0+ns): ``acc`` receives / accumulates h psi and may
-// alias pout_mf or pout.  ``ovl`` (optional) receives per-(state, y-plane)
-// partial sums [ns][n][2] of Re<psi|h psi> and Re<psi|pout> (without wxyz).
+// alias pout_mf or pout.  ``ovl`` (optional) receives per-state partial sums
+// [ns][hpsi_ovl_parts][2] of Re<psi|h psi> and Re<psi|pout> (without wxyz).
 int hpsi_launch(hfb_ctx_s* c, int prec, const void* pot, int s0, int ns, int nneut, const void* psi,
                 const double* weight, const double* weightuv, void* acc, void* pout, void* pout_mf, void* pout_del,
                 double* ovl, cudaStream_t st);
+
+// Single-precision hpsi on the tensor cores (hpsi_tc.cu): derivative
+// matrices built at context creation, availability, the launch (same
+// contract as hpsi_launch) and its number of overlap partials per state.
+int hpsi_tc_prepare(hfb_ctx_s* c);
+bool hpsi_tc_available(hfb_ctx_s* c, int prec);
+int hpsi_tc_parts(hfb_ctx_s* c);
+int hpsi_tc_launch(hfb_ctx_s* c, const void* pot, int s0, int ns, int nneut, const void* psi, const double* weight,
+                   const double* weightuv, void* acc, void* pout, void* pout_mf, void* pout_del, double* ovl,
+                   cudaStream_t st);
+
+// Partial sums per state that hpsi_launch writes into ``ovl``.
+int hpsi_ovl_parts(hfb_ctx_s* c, int prec);
 
 // (E0+T)^-1 preconditioner (levels.py:398-437) on states [0, ns):
 //  v = src - (use_lag ? lag : coef[s] * psi)     (plain src if psi == NULL)

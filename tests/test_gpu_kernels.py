@@ -94,10 +94,14 @@ def test_hpsi01_against_reference(unit, g8, dtype):
             assert rel(o, unit[f"hpsi_iq{iq}_{tag}"]) < tol, (iq, tag)
 
 
-@pytest.mark.parametrize("n,dtype", [(16, torch.complex128), (24, torch.complex128), (32, torch.complex64),
-                                     (48, torch.complex128), (48, torch.complex64), (40, torch.complex128)])
-def test_hpsi_batched_against_oracle(n, dtype):
-    """Batched hpsi over states of both isospins on larger grids vs the oracle."""
+@pytest.mark.parametrize("n,dtype,ns", [(16, torch.complex128, 5), (24, torch.complex128, 5),
+                                        (32, torch.complex64, 5), (48, torch.complex128, 5),
+                                        (48, torch.complex64, 5), (40, torch.complex128, 5),
+                                        (24, torch.complex64, 37), (40, torch.complex64, 6)])
+def test_hpsi_batched_against_oracle(n, dtype, ns):
+    """Batched hpsi over states of both isospins on larger grids vs the oracle
+    (single precision on 24-48 grids runs the tensor-core kernel; 37 states on
+    24^3 span several scheduling groups, the last one partial)."""
     import hfb
     from oracle import model, meanfield as omf
     rng = np.random.default_rng(n)
@@ -112,7 +116,7 @@ def test_hpsi_batched_against_oracle(n, dtype):
     mfo.v_pair = np.stack([-3 * w, -2 * w])
     for k, s in (("aq", 0.3), ("spot", 0.2), ("wlspot", 1.0)):
         setattr(mfo, k, s * rng.standard_normal((2, 3, 1, 1, 1)) * w[None, None])
-    ns, nn = 5, 3
+    nn = 3 if ns == 5 else ns // 2
     psi = (rng.standard_normal((ns, 2, n, n, n)) + 1j * rng.standard_normal((ns, 2, n, n, n))) * w
     wt = rng.uniform(0.2, 1.0, ns)
     wu = rng.uniform(0.0, 0.5, ns)
@@ -125,15 +129,18 @@ def test_hpsi_batched_against_oracle(n, dtype):
     pt = T(psi, dtype)
     out = torch.empty_like(pt)
     omf_ = torch.empty_like(pt)
+    odel = torch.empty_like(pt)
     wt_t, wu_t = T(wt), T(wu)          # keep the weight buffers alive across the launch
     from hfb._lib import call, ptr, stream_ptr, prec_of
     call("hfb_hpsi", gg.ctx.handle, prec_of(pt), ptr(mf.pot), ns, nn, ptr(pt), ptr(wt_t), ptr(wu_t), ptr(out),
-         ptr(omf_), None, stream_ptr())
+         ptr(omf_), ptr(odel), stream_ptr())
+    gg.ctx.check("hpsi")
     tol = 1e-11 if dtype == torch.complex128 else 1e-4
     for iq, sl in ((0, slice(0, nn)), (1, slice(nn, ns))):
         r = omf.hpsi01(g, mfo, iq, wt[sl], wu[sl], psi[sl])
         assert rel(out[sl], r[0]) < tol
         assert rel(omf_[sl], r[1]) < tol
+        assert rel(odel[sl], r[2]) < tol
 
 
 @pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
@@ -441,3 +448,26 @@ def test_eigh_near_diagonal(n, scale, kramers):
         assert np.max(np.abs(wv[k] - ref)) < 1e-12 * amax * n
         assert np.max(np.abs(a[k] @ vv[k] - vv[k] * wv[k][None, :])) < 1e-11 * amax
         assert np.max(np.abs(vv[k].conj().T @ vv[k] - np.eye(n))) < 1e-12
+
+
+@pytest.mark.gpu
+def test_single_precision_iterations_tensor_cores_match_cuda_cores(monkeypatch):
+    """Five single-precision iterations of O16 (24^3) with the tensor-core
+    kernels (hpsi, Gram, rotation) and with HFB_NO_TCGEN05=1 at context
+    creation (FFT hpsi and CUDA-core contractions) agree to single-precision
+    accuracy."""
+    from hfb import config, static
+
+    def run():
+        st = config.setup(config.case_dict("O16"), dtype=torch.complex64)
+        S = {k: st[k] for k in static._STATE_KEYS}
+        static.prepare(**S)
+        for i in range(1, 6):
+            static.iterate(i, **S)
+        return st["energies"].ehf, st["levels"].sp_energy.detach().cpu().numpy().copy()
+
+    e1, s1 = run()
+    monkeypatch.setenv("HFB_NO_TCGEN05", "1")
+    e2, s2 = run()
+    assert abs(e1 - e2) < 5e-3, (e1, e2)
+    assert np.max(np.abs(s1 - s2)) < 2e-2
