@@ -46,14 +46,15 @@ FALLBACK_HBM_GBS = 6650.0
 # Pb208 (measured with this bench's FP64 leg); scales the reference arm's
 # per-iteration CPU sample to a time-to-converge.
 PB208_FP64_ITERS = 675
-# DRAM bytes (read + write) per hpsi launch, both kernels, 236 FP32 states,
-# one output, from the ncu capture summarised in profiles/hpsi_pb208_fp32.md.
 # Both runs continue until the estimated remaining energy change is below
 # this (MeV): well past the 1 keV point that the time-to-converge reads, so
 # that the final states also carry converged single-particle energies for
 # the |d e_i| comparison.
-STOP_MEV = 5e-6
-HPSI_NCU_DRAM_BYTES = 426641664 + 376468224 + 839753216 + 373226752
+STOP_MEV = 1e-6
+# DRAM bytes (read + write) of one hpsi launch (hpsi_tc_kernel, 236 FP32
+# states, one output), from the ncu capture summarised in
+# profiles/hpsi_pb208_fp32.md.
+HPSI_NCU_DRAM_BYTES = 433642496 + 388209920
 
 
 def _peaks():
@@ -420,7 +421,7 @@ def main():
                     d_sp_energy_occupied_max_mev_vs_fp64=d_spe_occ,
                     fp64_ms_per_iteration=(r64["t"][-1] / r64["iters"] * 1e3)),
         roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
-                      traffic=HPSI_NCU_DRAM_BYTES, kernel="hpsi (hpsi_xplane + hpsi_yplane), FP32, 236 states",
+                      traffic=HPSI_NCU_DRAM_BYTES, kernel="hpsi (ht_fields_kernel + hpsi_tc_kernel, tcgen05), FP32, 236 states",
                       launch_ms=t_h * 1e3, bytes_per_launch=b_h, peak_kind=peak_kind),
         e2e=dict(value=e2e, unit=UNIT, h2d_bytes_per_step=rm["bytes_in"] / max(rm["iters"], 1),
                  d2h_bytes_per_step=rm["bytes_out"] / max(rm["iters"], 1)),
