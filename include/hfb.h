@@ -277,6 +277,42 @@ int hfb_energy_grad(hfb_ctx_t ctx, const hfb_force* f, const double* rho, const 
  * out[2..3] rms per isospin, out[4] total rms. */
 int hfb_rms(hfb_ctx_t ctx, const double* rho, double* out, void* stream);
 
+/* Density part of the nuclear observables, calculate_complete_observables
+ * (output.py:177-276) with calculate_isovector_dipoles (output.py:323-340):
+ * particle numbers, centres of mass, summed currents (pcm; zero when
+ * current == NULL), point rms radii and second moments about each isospin's
+ * own centre of mass, quadrupole tensors Q_ij = sum (3 x_i x_j - delta_ij
+ * r^2) rho dV, Q20 / Q22 from their eigenvalues, beta / gamma of the total
+ * tensor, the isovector Q20 (q20T1, with the nucleon numbers nneut, nprot)
+ * and the isovector dipole.  rho: [2][n^3] FP64; current: [2][3][n^3] FP64
+ * or NULL; out: HFB_NOBS doubles on the device, laid out as below
+ * (per-isospin arrays iq fastest, as the reference's (3, 2) shapes). */
+enum {
+  HFB_OBS_PNR = 0,        /* [2]          */
+  HFB_OBS_CM = 2,         /* [3][2]       */
+  HFB_OBS_PCM = 8,        /* [3][2]       */
+  HFB_OBS_RMS = 14,       /* [2]          */
+  HFB_OBS_X2M = 16,       /* [3][2]       */
+  HFB_OBS_Q20 = 22,       /* [2]          */
+  HFB_OBS_Q22 = 24,       /* [2]          */
+  HFB_OBS_PNRTOT = 26,
+  HFB_OBS_CMTOT = 27,     /* [3]          */
+  HFB_OBS_RMSTOT = 30,
+  HFB_OBS_X2MTOT = 31,    /* [3]          */
+  HFB_OBS_Q20TOT = 34,
+  HFB_OBS_Q22TOT = 35,
+  HFB_OBS_Q20T1 = 36,
+  HFB_OBS_BETA20 = 37,
+  HFB_OBS_BETA22 = 38,
+  HFB_OBS_BETA = 39,
+  HFB_OBS_GAMMA = 40,     /* degrees      */
+  HFB_OBS_DIPOLE = 41,    /* [3]          */
+  HFB_OBS_QMAT = 44,      /* [3][3][2]    */
+  HFB_NOBS = 62
+};
+int hfb_observables(hfb_ctx_t ctx, const double* rho, const double* current, double nneut, double nprot,
+                    double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

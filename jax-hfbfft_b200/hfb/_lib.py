@@ -89,6 +89,7 @@ _PROTOS = {
     "hfb_sum_energy": [vp, C.c_int] + [vp] * 6 + [vp, vp],
     "hfb_energy_grad": [vp, C.POINTER(HfbForce)] + [vp] * 5 + [vp, vp],
     "hfb_rms": [vp, vp, vp, vp],
+    "hfb_observables": [vp, vp, vp, C.c_double, C.c_double, vp, vp],
 }
 SYMBOLS = tuple(_PROTOS) + ("hfb_status_string", "hfb_launch_count", "hfb_last_cuda_error")
 

@@ -166,3 +166,61 @@ def rms_radii(dens, grids):
         rms[iq] = np.sqrt(np.sum(r2 * r) * w / pnr[iq])
     rmstot = np.sqrt((pnr[0] * rms[0] ** 2 + pnr[1] * rms[1] ** 2) / (pnr[0] + pnr[1]))
     return rms, rmstot
+
+
+def observables(rho, grids, nneut, nprot, current=None):
+    """Density part of calculate_complete_observables (output.py:177-276,
+    323-340): particle numbers, centres of mass, summed currents, point rms
+    radii and second moments about each isospin's own centre of mass, the
+    quadrupole tensors Q_ij = sum (3 x_i x_j - delta_ij r^2) rho dV, Q20 /
+    Q22 from their eigenvalues, the deformation beta / gamma and the
+    isovector dipole.  Returns a dict keyed by the reference's field names."""
+    w = grids.wxyz
+    coords = (grids.x[:, None, None], grids.y[None, :, None], grids.z[None, None, :])
+    pnr = np.zeros(2)
+    cm = np.zeros((3, 2))
+    pcm = np.zeros((3, 2))
+    rms = np.zeros(2)
+    x2m = np.zeros((3, 2))
+    qmat = np.zeros((3, 3, 2))
+    for iq in range(2):
+        r = rho[iq]
+        pnr[iq] = np.sum(r) * w
+        for d in range(3):
+            cm[d, iq] = np.sum(coords[d] * r) * w / pnr[iq]
+            if current is not None:
+                pcm[d, iq] = np.sum(current[iq, d]) * w
+        rel = [coords[d] - cm[d, iq] for d in range(3)]
+        r2 = rel[0] ** 2 + rel[1] ** 2 + rel[2] ** 2
+        rms[iq] = np.sqrt(np.sum(r2 * r) * w / pnr[iq])
+        for d in range(3):
+            x2m[d, iq] = np.sum(rel[d] ** 2 * r) * w / pnr[iq]
+        for i in range(3):
+            for j in range(3):
+                f = 3 * rel[i] ** 2 - r2 if i == j else 3 * rel[i] * rel[j]
+                qmat[i, j, iq] = np.sum(f * r) * w
+    pnrtot = pnr[0] + pnr[1]
+    cmtot = (pnr[0] * cm[:, 0] + pnr[1] * cm[:, 1]) / pnrtot
+    rmstot = np.sqrt((pnr[0] * rms[0] ** 2 + pnr[1] * rms[1] ** 2) / pnrtot)
+    x2mtot = (pnr[0] * x2m[:, 0] + pnr[1] * x2m[:, 1]) / pnrtot
+    c20, c22 = np.sqrt(5.0 / (16.0 * np.pi)), np.sqrt(5.0 / (96.0 * np.pi))
+    q20, q22 = np.zeros(2), np.zeros(2)
+    for iq in range(2):
+        ev = np.linalg.eigvalsh(qmat[:, :, iq])
+        q20[iq] = c20 * ev[2]
+        q22[iq] = c22 * (ev[1] - ev[0])
+    ev = np.linalg.eigvalsh(qmat[:, :, 0] + qmat[:, :, 1])
+    q20tot, q22tot = c20 * ev[2], c22 * (ev[1] - ev[0])
+    q20T1 = -q20[0] / nneut + q20[1] / nprot
+    scale = 4.0 * np.pi / (5.0 * rmstot ** 2 * pnrtot)
+    beta20tot, beta22tot = q20tot * scale, q22tot * scale
+    beta = np.sqrt(beta20tot ** 2 + 2.0 * beta22tot ** 2)
+    gamma = abs(np.arctan2(np.sqrt(2.0) * beta22tot, beta20tot)) * 180.0 / np.pi
+    if gamma > 120.0:
+        gamma -= 120.0
+    if 60.0 < gamma <= 120.0:
+        gamma = 120.0 - gamma
+    dip = np.array([np.sum(coords[d] * (rho[0] / pnr[0] - rho[1] / pnr[1])) * w for d in range(3)])
+    return dict(pnr=pnr, pnrtot=pnrtot, cm=cm, cmtot=cmtot, dipole_isovector=dip, rms=rms, rmstot=rmstot,
+                x2m=x2m, x2mtot=x2mtot, q20=q20, q22=q22, q20tot=q20tot, q22tot=q22tot, q20T1=q20T1,
+                beta20tot=beta20tot, beta22tot=beta22tot, beta=beta, gamma=gamma, pcm=pcm)

@@ -11,9 +11,12 @@ reference checkout)::
     python tests/golden/make_golden.py [--ref /root/reference]
 
 Outputs (committed): ``tests/golden/unit_n8.npz`` (per-function vectors on an
-8^3 grid with seeded random inputs) and ``tests/golden/run_<case>.npz``
+8^3 grid with seeded random inputs), ``tests/golden/run_<case>.npz``
 (end-to-end runs of the reference driver ``statichf_with_benchmark`` on small
-grids: per-iteration energies and final densities / levels).
+grids: per-iteration energies and final densities / levels) and
+``tests/golden/observables_n16.npz`` (``calculate_complete_observables`` on
+the runs' final densities and on a seeded triaxial density; needs the run
+fixtures, ``--only observables`` regenerates it alone).
 """
 import argparse
 import contextlib
@@ -228,6 +231,53 @@ def unit_vectors(m, ref):
     print(f"unit_n8: {len(out)} arrays")
 
 
+OBS_KEYS = ("pnr", "pnrtot", "cm", "cmtot", "dipole_isovector", "rms", "rmstot", "x2m", "x2mtot", "q20", "q22",
+            "q20tot", "q22tot", "q20T1", "beta20tot", "beta22tot", "beta", "gamma", "pcm")
+
+
+def observables_vectors(m, ref):
+    """output.calculate_complete_observables on the final densities of the
+    run fixtures (16^3) and on a seeded triaxial, off-centre density with
+    currents; the density part of the observables (particle numbers, centres
+    of mass, radii, second moments, quadrupole tensors, deformation,
+    isovector dipole, summed currents)."""
+    import types
+    import jax.numpy as jnp
+    out = {}
+    items = [(name, case, np.load(os.path.join(HERE, f"run_{name}.npz"))["rho"], None)
+             for name, case in RUN_CASES.items()]
+    rng = np.random.default_rng(20261204)
+    n = 16
+    tri = dict(grid=dict(nx=n, ny=n, nz=n, dx=1.0, dy=1.1, dz=0.9), force=dict(name="SLy4", ipair=0, tbcs=False),
+               levels=dict(nneut=12, nprot=10, npsi=[12, 10]),
+               static=dict(maxiter=1, radinx=2.0, radiny=2.0, radinz=2.0, serr=1e-20, x0dmp=0.2, e0dmp=100.0),
+               mprint=1)
+    h = np.array([1.0, 1.1, 0.9])
+    xs = [(np.arange(1, n + 1) - (n + 1) / 2) * h[d] for d in range(3)]
+    X, Y, Z = np.meshgrid(*xs, indexing="ij")
+    rho = np.stack([0.16 * np.exp(-((X - 0.4) / 3.1) ** 2 - ((Y + 0.3) / 2.6) ** 2 - ((Z - 0.2) / 3.8) ** 2),
+                    0.15 * np.exp(-((X - 0.3) / 3.0) ** 2 - ((Y + 0.2) / 2.7) ** 2 - ((Z - 0.1) / 3.6) ** 2)])
+    rho = rho * (1.0 + 0.05 * _smooth_random(rng, (2, n, n, n), n, 1.0))
+    cur = _smooth_random(rng, (2, 3, n, n, n), n, 0.01) + 0.002 * rng.normal(size=(2, 3, 1, 1, 1))
+    items.append(("triaxial_n16", tri, rho, cur))
+    for name, case, rho, cur in items:
+        params, forces, grids, dens, mf, levels, static, coul, en, moment, pairs = _setup(m, ref, case)
+        d = types.SimpleNamespace(rho=jnp.asarray(rho))
+        with contextlib.redirect_stdout(io.StringIO()):
+            obs = m["output"].calculate_complete_observables(d, levels, grids, params,
+                                                             None if cur is None else jnp.asarray(cur))
+        out[f"{name}_rho"] = np.asarray(rho)
+        if cur is not None:
+            out[f"{name}_current"] = np.asarray(cur)
+        out[f"{name}_grid"] = np.array([case["grid"]["nx"], case["grid"]["dx"], case["grid"]["dy"],
+                                        case["grid"]["dz"]])
+        out[f"{name}_nucleons"] = np.array([levels.nneut, levels.nprot], dtype=float)
+        for k in OBS_KEYS:
+            out[f"{name}_{k}"] = np.asarray(getattr(obs, k), dtype=float)
+    np.savez_compressed(os.path.join(HERE, "observables_n16.npz"), **out)
+    print(f"observables_n16: {len(items)} densities")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -236,6 +286,8 @@ def main():
     m = _import_reference(a.ref)
     if a.only in (None, "unit"):
         unit_vectors(m, a.ref)
+    if a.only in (None, "observables"):
+        observables_vectors(m, a.ref)
     for name, case in RUN_CASES.items():
         if a.only in (None, name):
             m = _import_reference(a.ref)

@@ -62,6 +62,12 @@ def test_fp64_run_matches_reference(name):
     pnr, rms, rmstot = hfb.output.rms_radii(dens, st["grids"])
     assert np.max(np.abs(np.array(rms) - ref["rms"])) < 1e-9
     assert abs(st["energies"].ehf - float(ref["ehf"])) < 1e-7
+    # deformation of the final state against the reference's observables
+    obs = dict(np.load(os.path.join(GOLDEN, "observables_n16.npz")))
+    o = hfb.output.calculate_complete_observables(dens, lv, st["grids"])
+    assert abs(o.rmstot - float(obs[f"{name}_rmstot"])) < 1e-9
+    assert np.max(np.abs(o.q20 - obs[f"{name}_q20"])) < 1e-6
+    assert abs(o.beta - float(obs[f"{name}_beta"])) < 1e-8
 
 
 @pytest.mark.parametrize("name", ["o16_n16", "ne20_vdi_n16"])

@@ -198,3 +198,38 @@ def test_run_matches_reference_driver(name):
     rms, rmstot = energies.rms_radii(rs.dens, rs.grids)
     assert np.max(np.abs(rms - ref["rms"])) < 1e-10
     assert abs(rs.en.ehf - ref["ehf"]) < 1e-8
+
+
+OBS_CASES = ("o16_n16", "ne20_vdi_n16", "o18_dddi_n16", "triaxial_n16")
+
+
+def obs_case(name):
+    """(oracle grids, rho, current or None, nneut, nprot, reference values)
+    of one density of tests/golden/observables_n16.npz."""
+    z = np.load(os.path.join(G, "observables_n16.npz"))
+    n, dx, dy, dz = z[f"{name}_grid"]
+    g = model.init_grids(int(n), int(n), int(n), dx, dy, dz)
+    cur = z[f"{name}_current"] if f"{name}_current" in z.files else None
+    nn, nz = z[f"{name}_nucleons"]
+    ref = {k[len(name) + 1:]: z[k] for k in z.files if k.startswith(name + "_")}
+    return g, z[f"{name}_rho"], cur, nn, nz, ref
+
+
+@pytest.mark.parametrize("name", OBS_CASES)
+def test_observables_oracle_against_reference(name):
+    """Moments, quadrupole deformation and dipole of the oracle against the
+    reference's calculate_complete_observables (output.py:177-340) on the
+    final densities of the golden runs and a triaxial density with currents.
+    gamma is compared only where the shape is deformed (beta > 0.01): for a
+    spherical density it is the angle of rounding noise."""
+    g, rho, cur, nn, nz, ref = obs_case(name)
+    o = energies.observables(rho, g, nn, nz, cur)
+    for k in ("pnr", "pnrtot", "cm", "cmtot", "dipole_isovector", "rms", "rmstot", "x2m", "x2mtot", "pcm"):
+        np.testing.assert_allclose(o[k], ref[k], rtol=1e-12, atol=1e-12, err_msg=k)
+    qs = max(1.0, float(np.max(np.abs(ref["q20"]))))
+    for k in ("q20", "q22", "q20tot", "q22tot"):
+        np.testing.assert_allclose(o[k], ref[k], rtol=0, atol=1e-11 * qs, err_msg=k)
+    for k in ("q20T1", "beta20tot", "beta22tot", "beta"):
+        np.testing.assert_allclose(o[k], ref[k], rtol=0, atol=1e-12, err_msg=k)
+    if ref["beta"] > 0.01:
+        assert abs(o["gamma"] - ref["gamma"]) < 1e-9
