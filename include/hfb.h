@@ -273,6 +273,14 @@ enum {
 int hfb_energy_grad(hfb_ctx_t ctx, const hfb_force* f, const double* rho, const double* tau,
                     const double* current, const double* sdens, const double* sodens,
                     double* out, void* stream);
+/* Single-particle orbital angular momentum, spin and parity (sp_properties,
+ * inout.py:64-150; the kinetic energy is hfb_sp_kinetic): orbital[nst][3],
+ * spin[nst][3], parity[nst] FP64 on the device (any may be NULL, not all),
+ * the orbital momentum about ``cm`` (host double[3], NULL for the origin),
+ * derivatives from the dense spectral matrices (cderv01), FP64 sums for
+ * FP64 or FP32 states.  Grids up to 64^3. */
+int hfb_sp_properties(hfb_ctx_t ctx, int prec, int nst, const void* psi, const double* cm, double* orbital,
+                      double* spin, double* parity, void* stream);
 /* Point rms radii (output.py:187-226, 246): out[0..1] particle numbers,
  * out[2..3] rms per isospin, out[4] total rms. */
 int hfb_rms(hfb_ctx_t ctx, const double* rho, double* out, void* stream);

@@ -1,4 +1,6 @@
-"""Radii and the density part of the nuclear observables (output.py:177-340)."""
+"""Radii, the nuclear observables (output.py:177-340) and the reference's
+.res output files (output.py:49-174)."""
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -27,10 +29,11 @@ HFB_NOBS = 62
 
 @dataclass
 class CompleteNuclearObservables:
-    """The reference's CompleteNuclearObservables (output.py) without the
-    angular-momentum fields, which need single-particle orbital and spin
-    expectation values this library does not compute; ``qmat`` (the
-    per-isospin quadrupole tensors, (3, 3, 2)) is added."""
+    """The reference's CompleteNuclearObservables (output.py:8-46) plus
+    ``qmat``, the per-isospin quadrupole tensors (3, 3, 2).  The angular
+    momenta are the occupation-weighted sums of the levels' single-particle
+    orbital and spin expectation values (output.py:297-320); they are zero
+    while nothing has filled ``levels.sp_orbital`` / ``sp_spin``."""
     pnr: np.ndarray
     pnrtot: float
     cm: np.ndarray
@@ -51,6 +54,9 @@ class CompleteNuclearObservables:
     gamma: float
     pcm: np.ndarray
     qmat: np.ndarray
+    orbital_momentum: np.ndarray = None
+    spin_momentum: np.ndarray = None
+    total_momentum: np.ndarray = None
 
 
 def observables_raw(grids, rho, nneut, nprot, current=None):
@@ -75,4 +81,96 @@ def calculate_complete_observables(densities, levels, grids, params=None, curren
         n = int(np.prod(shp)) if shp else 1
         x = v[o:o + n]
         vals[k] = float(x[0]) if not shp else x.reshape(shp).copy()
+    vals["orbital_momentum"], vals["spin_momentum"] = angular_momentum(levels)
+    vals["total_momentum"] = vals["orbital_momentum"] + vals["spin_momentum"]
     return CompleteNuclearObservables(**vals)
+
+
+def angular_momentum(levels):
+    """Occupation-weighted sums of the single-particle orbital and spin
+    expectation values over states with wocc > 1e-10 (output.py:297-320);
+    zeros for levels without them."""
+    orb, spin = getattr(levels, "sp_orbital", None), getattr(levels, "sp_spin", None)
+    if orb is None or spin is None:
+        return np.zeros(3), np.zeros(3)
+    w = levels.wocc * levels.wstates * (levels.wocc > 1e-10)
+    orb = orb if orb.shape[-1] == 3 else orb.T   # (nst, 3)
+    spin = spin if spin.shape[-1] == 3 else spin.T
+    return (w[:, None] * orb).sum(0).cpu().numpy(), (w[:, None] * spin).sum(0).cpu().numpy()
+
+
+class FortranOutputWriter:
+    """The reference's per-iteration .res files (output.py:49-174): the same
+    file names, header lines and column formats, so that tools reading the
+    reference's (and the Fortran code's) output read these.  Files are
+    created with their headers when the writer is made and get one line per
+    ``write_iteration_data`` call."""
+
+    HEADERS = {
+        "conver": "# Iter   Energy  d_Energy    sp_fluct    max(lam-)     rms(lam-)      rms    "
+                  "beta2  gamma      x_0     e_pair(1)    e_pair(2)\n",
+        "energies": "# Iter    N(n)    N(p)       E(sum)         E(integ)       Ekin         "
+                    "E_Coul         ehfCrho0       ehfCrho1       ehfCdrho0      ehfCdrho1     "
+                    "ehfCtau0       ehfCtau1       ehfCdJ0        ehfCdJ1       e_pair(1)    "
+                    "e_pair(2)      e_zpe\n",
+        "dipoles": "# Iter    c.m. x-y-z                                  Isovector dipoles x-y-z\n",
+        "spin": "# Iter      Lx        Ly        Lz        Sx        Sy        Sz        Jx        Jy        Jz\n",
+        "monopoles": "# Iter    RMS_n     RMS_p     RMS_tot   RMS_diff   N_dens    Z_dens    A_dens\n",
+        "quadrupoles": "# Iter    Q20_n     Q20_p     Q20_tot   Q22_tot   <x\u00b2>_tot  <y\u00b2>_tot  "
+                       "<z\u00b2>_tot  Beta      Gamma\n",
+        "momenta": "# Iter    Px_n      Py_n      Pz_n      Px_p      Py_p      Pz_p      "
+                   "Px_tot    Py_tot    Pz_tot\n",
+    }
+
+    def __init__(self, output_dir):
+        self.output_dir = output_dir
+        os.makedirs(output_dir, exist_ok=True)
+        self.files = {k: os.path.join(output_dir, f"{k}.res") for k in self.HEADERS}
+        for k, h in self.HEADERS.items():
+            with open(self.files[k], "w", encoding="utf-8") as f:
+                f.write(h)
+
+    def _append(self, key, text):
+        with open(self.files[key], "a", encoding="utf-8") as f:
+            f.write(text + "\n")
+
+    def write_iteration_data(self, iteration, energies, observables, static, pairs):
+        en, ob, ep = energies, observables, pairs.epair
+        de = 0.0
+        if getattr(en, "ehfprev", 0.0) != 0.0 and iteration > 0:
+            de = en.ehf - en.ehfprev
+        f1, f2 = en.efluct1[0], en.efluct2[0]
+        self._append("conver", f"{iteration:4d} {en.ehf:12.6f} {de:12.6f} {f1:12.6e} {f1:12.6e} {f2:12.6e} "
+                               f"{ob.rmstot:8.4f} {ob.beta:8.4f} {ob.gamma:8.2f} {static.x0dmp:8.4f} "
+                               f"{ep[0]:12.6f} {ep[1]:12.6f}")
+        cols = [en.ehfCrho0, en.ehfCrho1, en.ehfCdrho0, en.ehfCdrho1, en.ehfCtau0, en.ehfCtau1, en.ehfCdJ0,
+                en.ehfCdJ1, ep[0], ep[1], en.e_zpe]
+        self._append("energies", f"{iteration:4d} {ob.pnr[0]:8.2f} {ob.pnr[1]:8.2f} {en.ehf:14.6f} "
+                                 f"{en.ehfint:14.6f} {en.tke:12.6f} {en.ehfc:12.6f} "
+                                 + " ".join(f"{c:12.6f}" for c in cols))
+        self._append("dipoles", f"{iteration:4d} " + " ".join(f"{c:12.6f}" for c in list(ob.cmtot[:3])
+                                                             + list(ob.dipole_isovector[:3])))
+        mom = list(ob.orbital_momentum[:3]) + list(ob.spin_momentum[:3]) + list(ob.total_momentum[:3])
+        self._append("spin", f"{iteration:4d} " + " ".join(f"{c:10.6f}" for c in mom))
+        self._append("monopoles", f"{iteration:4d} {ob.rms[0]:9.6f} {ob.rms[1]:9.6f} {ob.rmstot:9.6f} "
+                                  f"{ob.rms[0] - ob.rms[1]:9.6f} {ob.pnr[0]:9.3f} {ob.pnr[1]:9.3f} "
+                                  f"{ob.pnrtot:9.3f}")
+        self._append("quadrupoles", f"{iteration:4d} " + " ".join(
+            f"{c:9.6f}" for c in [ob.q20[0], ob.q20[1], ob.q20tot, ob.q22tot, ob.x2mtot[0], ob.x2mtot[1],
+                                  ob.x2mtot[2], ob.beta]) + f" {ob.gamma:9.2f}")
+        p = np.asarray(ob.pcm)
+        self._append("momenta", f"{iteration:4d} " + " ".join(
+            f"{c:10.6f}" for c in [p[0, 0], p[1, 0], p[2, 0], p[0, 1], p[1, 1], p[2, 1], p[0, 0] + p[0, 1],
+                                  p[1, 0] + p[1, 1], p[2, 0] + p[2, 1]]))
+
+
+def res_callback(state, writer, current=False):
+    """A ``callback(i, energies)`` for hfb.static.statichf that appends one
+    line per iteration to the .res files of ``writer``, as the reference's
+    statichf_with_benchmark does with an output writer (static.py:1721-1733,
+    complete_sinfo_with_fortran_output)."""
+    def cb(i, energies):
+        obs = calculate_complete_observables(state["densities"], state["levels"], state["grids"], state["params"],
+                                             state["densities"].current if current else None)
+        writer.write_iteration_data(i, energies, obs, state["static"], state["pairs"])
+    return cb

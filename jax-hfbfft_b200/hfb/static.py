@@ -180,9 +180,12 @@ def _energies(coulomb, densities, energies, forces, grids, levels, meanfield, pa
 
 
 def prepare(coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs):
-    """Steps before the loop (static.py:1700-1744)."""
-    params.iteration = 0
-    diagstep(energies, forces, grids, levels, static, False, True)
+    """Steps before the loop (static.py:1700-1744).  With params.trestart
+    (states loaded by hfb.restart.load_state) the first diagonalisation is
+    skipped and params.iteration is kept, as in static.py:1700-1704."""
+    if not params.trestart:
+        params.iteration = 0
+        diagstep(energies, forces, grids, levels, static, False, True)
     add_density(densities, grids, levels)
     skyrme(coulomb, densities, forces, grids, meanfield, params, static, dtype=levels.psi.dtype)
     grstep(forces, grids, levels, meanfield, params, static)
@@ -239,6 +242,12 @@ def iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, p
     return False
 
 
+def first_iteration(params):
+    """First loop index: 1, or the saved iteration + 1 on a restart
+    (static.py:1700-1701)."""
+    return params.iteration + 1 if params.trestart else 1
+
+
 def statichf(coulomb, densities, energies, forces, grids, levels, meanfield, moment, params, static, pairs,
              maxiter=None, x0_schedule=None, callback=None, de_tol=None):
     """The self-consistent loop (static.py:1666-1882, without file output).
@@ -251,10 +260,11 @@ def statichf(coulomb, densities, energies, forces, grids, levels, meanfield, mom
     t0 = time.perf_counter()
     prepare(coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs)
     energies.sync()
-    res.history.append(dict(iteration=0, ehf=energies.ehf, ehfint=energies.ehfint, x0dmp=static.x0dmp))
+    res.history.append(dict(iteration=first_iteration(params) - 1, ehf=energies.ehf, ehfint=energies.ehfint,
+                            x0dmp=static.x0dmp))
     n = static.maxiter if maxiter is None else maxiter
     prev = energies.ehf
-    for i in range(1, n + 1):
+    for i in range(first_iteration(params), n + 1):
         x0_used = static.x0dmp
         done = iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs,
                        x0_schedule)

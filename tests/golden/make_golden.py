@@ -16,7 +16,9 @@ Outputs (committed): ``tests/golden/unit_n8.npz`` (per-function vectors on an
 grids: per-iteration energies and final densities / levels) and
 ``tests/golden/observables_n16.npz`` (``calculate_complete_observables`` on
 the runs' final densities and on a seeded triaxial density; needs the run
-fixtures, ``--only observables`` regenerates it alone).
+fixtures, ``--only observables`` regenerates it alone) and
+``tests/golden/res_files.json`` (the text of the reference's .res writers
+for seeded inputs, ``--only res``).
 """
 import argparse
 import contextlib
@@ -278,6 +280,52 @@ def observables_vectors(m, ref):
     print(f"observables_n16: {len(items)} densities")
 
 
+def res_writer_vectors(m, ref):
+    """Text written by the reference's FortranOutputWriter (output.py:49-174)
+    for three iterations of seeded synthetic energies, observables, damping
+    and pairing values; the inputs are stored beside the file contents."""
+    import json
+    import types
+    rng = np.random.default_rng(20261205)
+    iters = []
+    prev = 0.0
+    for it in range(3):
+        en = {k: float(rng.normal(0.0, 50.0)) for k in
+              ("ehf", "ehfint", "tke", "ehfc", "ehfCrho0", "ehfCrho1", "ehfCdrho0", "ehfCdrho1", "ehfCtau0",
+               "ehfCtau1", "ehfCdJ0", "ehfCdJ1", "e_zpe")}
+        en["ehfprev"] = prev
+        en["efluct1"] = [float(abs(rng.normal(0.0, 1e-3)))]
+        en["efluct2"] = [float(abs(rng.normal(0.0, 1e-3)))]
+        prev = en["ehf"]
+        ob = dict(pnr=rng.uniform(5, 90, 2).tolist(), cmtot=rng.normal(0, 1e-3, 3).tolist(),
+                  dipole_isovector=rng.normal(0, 1e-2, 3).tolist(), orbital_momentum=rng.normal(0, 1, 3).tolist(),
+                  spin_momentum=rng.normal(0, 0.5, 3).tolist(), rms=rng.uniform(2, 6, 2).tolist(),
+                  q20=rng.normal(0, 30, 2).tolist(), x2mtot=rng.uniform(1, 20, 3).tolist(),
+                  pcm=rng.normal(0, 1e-2, (3, 2)).tolist())
+        ob["total_momentum"] = (np.array(ob["orbital_momentum"]) + np.array(ob["spin_momentum"])).tolist()
+        ob["pnrtot"] = ob["pnr"][0] + ob["pnr"][1]
+        for k in ("rmstot", "q20tot", "q22tot", "beta"):
+            ob[k] = float(abs(rng.normal(0, 3)))
+        ob["gamma"] = float(rng.uniform(0, 60))
+        iters.append(dict(iteration=it, energies=en, observables=ob, x0dmp=float(rng.uniform(0.1, 0.9)),
+                          epair=rng.normal(-5, 2, 2).tolist()))
+    tmp = tempfile.mkdtemp()
+    w = m["output"].FortranOutputWriter(tmp)
+    for d in iters:
+        en = types.SimpleNamespace(**d["energies"])
+        ob = types.SimpleNamespace(**{k: (np.array(v) if isinstance(v, list) else v)
+                                      for k, v in d["observables"].items()})
+        w.write_iteration_data(d["iteration"], en, ob, types.SimpleNamespace(x0dmp=d["x0dmp"]),
+                               types.SimpleNamespace(epair=np.array(d["epair"])))
+    files = {}
+    for k, path in w.files.items():
+        with open(path) as f:
+            files[os.path.basename(path)] = f.read()
+    with open(os.path.join(HERE, "res_files.json"), "w") as f:
+        json.dump(dict(inputs=iters, files=files), f, indent=1)
+    print(f"res_files: {len(files)} files")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -288,6 +336,8 @@ def main():
         unit_vectors(m, a.ref)
     if a.only in (None, "observables"):
         observables_vectors(m, a.ref)
+    if a.only in (None, "res"):
+        res_writer_vectors(m, a.ref)
     for name, case in RUN_CASES.items():
         if a.only in (None, name):
             m = _import_reference(a.ref)

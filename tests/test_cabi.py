@@ -136,3 +136,24 @@ def test_force_jacobian_matches_finite_differences():
         for b in ("b0", "b0p", "b1", "b1p", "b2", "b2p", "b3", "b3p", "b4", "b4p"):
             d = (getattr(fp, b) - getattr(fm, b)) / (2 * h)
             assert d == pytest.approx(row.get(b, 0.0), rel=1e-6, abs=1e-9), (name, b)
+
+
+def test_res_writer_matches_reference_text(tmp_path):
+    """hfb.output.FortranOutputWriter writes the same bytes as the
+    reference's writer (output.py:49-174) for the seeded inputs of
+    tests/golden/res_files.json."""
+    import json
+    import types
+    import numpy as np
+    from hfb.output import FortranOutputWriter
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "res_files.json")))
+    w = FortranOutputWriter(str(tmp_path))
+    for it in d["inputs"]:
+        en = types.SimpleNamespace(**it["energies"])
+        ob = types.SimpleNamespace(**{k: (np.array(v) if isinstance(v, list) else v)
+                                      for k, v in it["observables"].items()})
+        w.write_iteration_data(it["iteration"], en, ob, types.SimpleNamespace(x0dmp=it["x0dmp"]),
+                               types.SimpleNamespace(epair=np.array(it["epair"])))
+    for name, text in d["files"].items():
+        with open(os.path.join(tmp_path, name), encoding="utf-8") as f:
+            assert f.read() == text, name

@@ -164,6 +164,14 @@ def test_kinetic_energy_against_reference(unit, g8):
     lv.psi.copy_(T(unit["in_dens_psi"]))
     hfb.inout.sp_properties(f, g8, lv)
     assert rel(lv.sp_kinetic, unit["spp_sp_kinetic"]) < TOL64
+    # orbital angular momentum, spin, parity (hfb_sp_properties)
+    for k in ("sp_orbital", "sp_spin", "sp_parity"):
+        assert rel(getattr(lv, k), unit[f"spp_{k}"]) < 1e-12, k
+    lv32 = hfb.levels.init_levels(g8, 3, 2, (4, 3), dtype=torch.complex64)
+    lv32.psi.copy_(T(unit["in_dens_psi"], torch.complex64))
+    hfb.inout.sp_properties(f, g8, lv32)
+    for k in ("sp_orbital", "sp_spin", "sp_parity"):
+        assert rel(getattr(lv32, k), unit[f"spp_{k}"]) < 1e-5, k
     # the fused path inside add_density gives the same numbers
     for k in ("wocc", "wguv", "pairwg", "wstates"):
         getattr(lv, k).copy_(T(unit[f"in_dens_{k}"]))
