@@ -281,6 +281,32 @@ int hfb_energy_grad(hfb_ctx_t ctx, const hfb_force* f, const double* rho, const 
  * FP64 or FP32 states.  Grids up to 64^3. */
 int hfb_sp_properties(hfb_ctx_t ctx, int prec, int nst, const void* psi, const double* cm, double* orbital,
                       double* spin, double* parity, void* stream);
+/* Quadrupole / principal-axis constraints (constraint.py:47-342; the
+ * reference defines them but does not call them from its driver).  Field
+ * kinds (constraint.py:126-184, stacked in this order): Q20 (1 field), Q22
+ * (1), principal axes (6: xy, xz, yz, x, y, z).  Fields are masked by
+ * 1 / (1 + exp((r - damprad) / dampgamma)), normalised by r0rms^2 A^(5/3),
+ * act on both isospins alike and are stored [nc][n^3] FP64 on the device.
+ *   hfb_constraint_fields     the fields of ``kinds`` (bitwise or)
+ *   hfb_constraint_moments    out[c] = <Q_c> = dV sum Q_c (rho_n + rho_p),
+ *                             out[nc + c] = |<Q_c^2> - <Q_c>^2 / N|,
+ *                             out[2 nc] = N (device, 2 nc + 1 doubles)
+ *   hfb_constraint_potential  upot_q -= sum lambda_c Q_c (FP64 [2][n^3]) and
+ *                             the same on field 0 of the packed hpsi
+ *                             potentials ``pot`` [2][12][n^3] in ``prec``
+ *                             (either may be NULL); lambda: host [nc]
+ *   hfb_constraint_correct    psi_s *= exp(wstates_s wocc_s (-sum qcorr_c
+ *                             Q_c)) on both spin components; qcorr: host [nc]
+ */
+enum { HFB_CON_Q20 = 1, HFB_CON_Q22 = 2, HFB_CON_PRINCIPAL = 4, HFB_CON_MAX = 8 };
+int hfb_constraint_fields(hfb_ctx_t ctx, int kinds, double mass_number, double r0rms, double damprad,
+                          double dampgamma, double* fields, void* stream);
+int hfb_constraint_moments(hfb_ctx_t ctx, int nc, const double* fields, const double* rho, double* out,
+                           void* stream);
+int hfb_constraint_potential(hfb_ctx_t ctx, int prec, int nc, const double* fields, const double* lambda,
+                             double* upot, void* pot, void* stream);
+int hfb_constraint_correct(hfb_ctx_t ctx, int prec, int nst, int nc, const double* fields, const double* qcorr,
+                           const double* wocc, const double* wstates, void* psi, void* stream);
 /* Point rms radii (output.py:187-226, 246): out[0..1] particle numbers,
  * out[2..3] rms per isospin, out[4] total rms. */
 int hfb_rms(hfb_ctx_t ctx, const double* rho, double* out, void* stream);

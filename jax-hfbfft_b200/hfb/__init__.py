@@ -12,6 +12,6 @@ include/hfb.h; importing works without a GPU, computing does not.
 """
 from . import _lib  # noqa: F401
 from . import params, forces, grids, levels, meanfield, densities, coulomb, pairs, energies, inout  # noqa: F401
-from . import static, output, config, adjoint, batch, restart  # noqa: F401
+from . import static, output, config, adjoint, batch, restart, constraint  # noqa: F401
 
 __version__ = "0.1.0"

@@ -91,6 +91,10 @@ _PROTOS = {
     "hfb_rms": [vp, vp, vp, vp],
     "hfb_observables": [vp, vp, vp, C.c_double, C.c_double, vp, vp],
     "hfb_sp_properties": [vp, C.c_int, C.c_int, vp, C.POINTER(C.c_double), vp, vp, vp, vp],
+    "hfb_constraint_fields": [vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, vp, vp],
+    "hfb_constraint_moments": [vp, C.c_int, vp, vp, vp, vp],
+    "hfb_constraint_potential": [vp, C.c_int, C.c_int, vp, C.POINTER(C.c_double), vp, vp, vp],
+    "hfb_constraint_correct": [vp, C.c_int, C.c_int, C.c_int, vp, C.POINTER(C.c_double), vp, vp, vp, vp],
 }
 SYMBOLS = tuple(_PROTOS) + ("hfb_status_string", "hfb_launch_count", "hfb_last_cuda_error")
 

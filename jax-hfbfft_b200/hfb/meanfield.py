@@ -75,9 +75,10 @@ def hpsi01(grids, meanfield, iq, weight, weightuv, pinn):
 
 
 def skyrme(coulomb, densities, forces, grids, meanfield, params, static, constraints=None, dtype=None):
-    """Potentials from densities (meanfield.py:164-391), on the device."""
-    if constraints is not None:
-        raise NotImplementedError("constraints are not wired in the reference (meanfield.py:246-248)")
+    """Potentials from densities (meanfield.py:164-391), on the device.
+    With ``constraints`` (hfb.constraint.Constraints) the constraint
+    potential is subtracted from upot afterwards, where meanfield.py:246-248
+    leaves the place for it."""
     if getattr(static, "outertype", "N") != "N":
         raise NotImplementedError(f"outertype '{static.outertype}' not implemented.")
     if dtype is None:
@@ -92,4 +93,7 @@ def skyrme(coulomb, densities, forces, grids, meanfield, params, static, constra
          ptr(d.sdens), ptr(d.sodens), ptr(m.upot), ptr(m.bmass), ptr(m.divaq), ptr(m.v_pair), ptr(m.aq),
          ptr(m.spot), ptr(m.wlspot), ptr(m.dbmass), ptr(coulomb.wcoul), ptr(m.ecorrp_dev),
          HFB_F64 if rd == torch.float64 else HFB_F32, ptr(m.pot), stream_ptr())
+    if constraints is not None:
+        from .constraint import add_constraint_potential
+        add_constraint_potential(meanfield, constraints, grids)
     return meanfield, coulomb

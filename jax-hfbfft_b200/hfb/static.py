@@ -51,6 +51,7 @@ class Static:
     symcond: torch.Tensor = None
     lambda_save: torch.Tensor = None
     sums_dev: torch.Tensor = None      # running sumflu, delesum on the device
+    constraints: object = None         # hfb.constraint.Constraints, or None (unconstrained)
 
     @property
     def sumflu(self):
@@ -179,6 +180,11 @@ def _energies(coulomb, densities, energies, forces, grids, levels, meanfield, pa
     return energies
 
 
+def _active_constraints(static):
+    c = getattr(static, "constraints", None)
+    return c if c is not None and c.tconstraint else None
+
+
 def prepare(coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs):
     """Steps before the loop (static.py:1700-1744).  With params.trestart
     (states loaded by hfb.restart.load_state) the first diagonalisation is
@@ -187,7 +193,13 @@ def prepare(coulomb, densities, energies, forces, grids, levels, meanfield, para
         params.iteration = 0
         diagstep(energies, forces, grids, levels, static, False, True)
     add_density(densities, grids, levels)
-    skyrme(coulomb, densities, forces, grids, meanfield, params, static, dtype=levels.psi.dtype)
+    cons = _active_constraints(static)
+    if cons is not None:
+        from .constraint import calculate_constraint_expectation_values
+        ex, var = calculate_constraint_expectation_values(densities, cons, grids)
+        static.constraints = cons.replace(actual_crank=ex, actual_crank2=var)
+    skyrme(coulomb, densities, forces, grids, meanfield, params, static, constraints=_active_constraints(static),
+           dtype=levels.psi.dtype)
     grstep(forces, grids, levels, meanfield, params, static)
     if forces.ipair != 0:
         pair(levels, meanfield, forces, params, grids, pairs)
@@ -209,6 +221,10 @@ def iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, p
     params.iteration = i
     forces.tbcs = True if i <= static.inibcs else static._tbcssav
     static.tdiag = not (i > static.inidiag)
+    cons = _active_constraints(static)
+    if cons is not None:
+        from .constraint import before_constraint_step
+        static.constraints = before_constraint_step(cons)
     grstep(forces, grids, levels, meanfield, params, static)
     if forces.tbcs:
         static.tdiag = True
@@ -220,7 +236,14 @@ def iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, p
     # densities with mixing 0.2 new + 0.8 old for rho, tau, chi, and the
     # kinetic energies of sp_properties from the same derivatives
     add_density(densities, grids, levels, mix=0.2, forces=forces)
-    skyrme(coulomb, densities, forces, grids, meanfield, params, static, dtype=levels.psi.dtype)
+    if cons is not None:
+        # multipliers from the new densities, correction of the states
+        # (constraint.py:324-351), potential added after skyrme
+        from .constraint import tune_constraints
+        static.constraints, _ = tune_constraints(static.constraints, densities, levels, grids, static.e0dmp,
+                                                 static.x0dmp)
+    skyrme(coulomb, densities, forces, grids, meanfield, params, static, constraints=_active_constraints(static),
+           dtype=levels.psi.dtype)
     _energies(coulomb, densities, energies, forces, grids, levels, meanfield, params, pairs)
     energies.sync()
     grids.ctx.check(f"iteration {i}")

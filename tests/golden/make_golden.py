@@ -18,7 +18,8 @@ grids: per-iteration energies and final densities / levels) and
 the runs' final densities and on a seeded triaxial density; needs the run
 fixtures, ``--only observables`` regenerates it alone) and
 ``tests/golden/res_files.json`` (the text of the reference's .res writers
-for seeded inputs, ``--only res``).
+for seeded inputs, ``--only res``) and ``tests/golden/constraint_n16.npz``
+(the reference's constraint module on seeded inputs, ``--only constraint``).
 """
 import argparse
 import contextlib
@@ -41,7 +42,7 @@ def _import_reference(ref):
     import jax  # noqa: F401  (the stand-in)
     mods = {}
     for name in ("params", "forces", "grids", "densities", "meanfield", "levels", "static",
-                 "coulomb", "moment", "energies", "pairs", "output", "inout", "trivial"):
+                 "coulomb", "moment", "energies", "pairs", "output", "inout", "trivial", "constraint"):
         mods[name] = __import__(name)
     return mods
 
@@ -326,6 +327,53 @@ def res_writer_vectors(m, ref):
     print(f"res_files: {len(files)} files")
 
 
+def constraint_vectors(m, ref):
+    """The reference's constraint module (constraint.py:47-342; not wired
+    into its driver) on a 16^3 grid: the constraint fields for Q20 + Q22 +
+    principal axes, expectation values and variances of a seeded density,
+    one multiplier update, the wave-function correction of seeded states
+    and the constraint potential."""
+    import types
+    import jax.numpy as jnp
+    c = __import__("constraint")
+    n = 16
+    case = dict(grid=dict(nx=n, ny=n, nz=n, dx=1.0, dy=1.0, dz=1.0), force=dict(name="SLy4", ipair=0, tbcs=False),
+                levels=dict(nneut=8, nprot=8, npsi=[5, 4]),
+                static=dict(maxiter=1, radinx=2.0, radiny=2.0, radinz=2.0, serr=1e-20, x0dmp=0.2, e0dmp=100.0),
+                mprint=1)
+    params, forces, grids, dens, mf, levels, static, coul, en, moment, pairs = _setup(m, ref, case)
+    rng = np.random.default_rng(20261206)
+    with contextlib.redirect_stdout(io.StringIO()):
+        cs = c.init_constraints(dict(alpha20_wanted=0.3, alpha22_wanted=0.05, tq_prin_axes=True), 16, grids)
+    X, Y, Z = np.meshgrid(grids.x, grids.y, grids.z, indexing="ij")
+    rho = np.stack([0.16 * np.exp(-(X / 2.8) ** 2 - (Y / 2.6) ** 2 - (Z / 3.3) ** 2),
+                    0.15 * np.exp(-(X / 2.7) ** 2 - (Y / 2.6) ** 2 - (Z / 3.2) ** 2)])
+    d = types.SimpleNamespace(rho=jnp.asarray(rho))
+    ex, var = c.calculate_constraint_expectation_values(d, cs, grids)
+    cs = cs.replace(old_crank=jnp.asarray(np.asarray(ex) * 0.9))
+    cs2 = c.update_lagrange_multipliers(cs, ex, var, 100.0, 0.2)
+    ns = 9
+    psi = rng.normal(size=(ns, 2, n, n, n)) + 1j * rng.normal(size=(ns, 2, n, n, n))
+    iso = np.array([1] * 5 + [2] * 4)
+    wocc = rng.uniform(0.2, 1.0, ns)
+    wst = np.ones(ns)
+    lv = types.SimpleNamespace(isospin=jnp.asarray(iso), wocc=jnp.asarray(wocc), wstates=jnp.asarray(wst))
+    # the reference's correction indexes fields [x, y, z, isospin] and
+    # multiplies a spinor laid out [2, x, y, z] by [x, y, z, None]; it is
+    # applied here to states stored [x, y, z, 2], the layout it indexes
+    psi_xyzs = np.moveaxis(psi, 1, -1)
+    cor = c.apply_wavefunction_corrections(jnp.asarray(psi_xyzs), cs2, lv)
+    upot = rng.normal(size=(n, n, n, 2))
+    pot = c.add_constraint_potential(jnp.asarray(upot), cs2)
+    out = dict(rho=rho, fields=np.asarray(cs.constr_field), goals=np.asarray(cs.goal_crank),
+               lambda0=np.asarray(cs.lambda_crank), old=np.asarray(cs.old_crank), expect=np.asarray(ex),
+               var=np.asarray(var), lambda1=np.asarray(cs2.lambda_crank), qcorr=np.asarray(cs2.qcorr),
+               psi=psi, isospin=iso, wocc=wocc, wstates=wst, psi_corrected=np.moveaxis(np.asarray(cor), -1, 1),
+               upot_xyzs=upot, pot_xyzs=np.asarray(pot), mass_number=16.0)
+    np.savez_compressed(os.path.join(HERE, "constraint_n16.npz"), **out)
+    print(f"constraint_n16: {cs.numconstraint} constraints")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -338,6 +386,8 @@ def main():
         observables_vectors(m, a.ref)
     if a.only in (None, "res"):
         res_writer_vectors(m, a.ref)
+    if a.only in (None, "constraint"):
+        constraint_vectors(m, a.ref)
     for name, case in RUN_CASES.items():
         if a.only in (None, name):
             m = _import_reference(a.ref)

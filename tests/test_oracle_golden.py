@@ -233,3 +233,27 @@ def test_observables_oracle_against_reference(name):
         np.testing.assert_allclose(o[k], ref[k], rtol=0, atol=1e-12, err_msg=k)
     if ref["beta"] > 0.01:
         assert abs(o["gamma"] - ref["gamma"]) < 1e-9
+
+
+def test_constraint_oracle_against_reference():
+    """The constraint restatement (oracle/constraint.py) against the
+    reference's constraint.py functions on seeded inputs: fields, moments,
+    one multiplier update, the state correction and the potential."""
+    from oracle import constraint as oc
+    z = np.load(os.path.join(G, "constraint_n16.npz"))
+    g = model.init_grids(16, 16, 16, 1.0, 1.0, 1.0)
+    f, names = oc.constraint_fields(g, oc.Q20 | oc.Q22 | oc.PRINCIPAL, float(z["mass_number"]))
+    assert names == ["q20", "q22", "xy", "xz", "yz", "x", "y", "z"]
+    ref_f = np.moveaxis(z["fields"], -1, 1)              # [i][iq][x][y][z]
+    np.testing.assert_allclose(f, ref_f[:, 0], rtol=0, atol=1e-15)
+    np.testing.assert_array_equal(ref_f[:, 0], ref_f[:, 1])
+    ex, var = oc.expectation_values(f, z["rho"], g.wxyz)
+    np.testing.assert_allclose(ex, z["expect"], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(var, z["var"], rtol=1e-12, atol=1e-15)
+    lam, qc = oc.update_multipliers(z["lambda0"], z["old"], z["goals"], z["expect"], z["var"], 100.0, 0.2)
+    np.testing.assert_allclose(lam, z["lambda1"], rtol=1e-13)
+    np.testing.assert_allclose(qc, z["qcorr"], rtol=1e-13, atol=1e-16)
+    cor = oc.correct_states(z["psi"], f, z["qcorr"], z["isospin"] - 1, z["wocc"], z["wstates"])
+    assert rel(cor, z["psi_corrected"]) < 1e-13
+    pot = oc.constraint_potential(np.moveaxis(z["upot_xyzs"], -1, 0), f, z["lambda1"])
+    assert rel(pot, np.moveaxis(z["pot_xyzs"], -1, 0)) < 1e-14
