@@ -52,8 +52,8 @@ PB208_FP64_ITERS = 675
 # the |d e_i| comparison.
 STOP_MEV = 1e-6
 # DRAM bytes (read + write) of one hpsi launch (hpsi_tc_kernel, 236 FP32
-# states, one output), from the ncu capture summarised in
-# profiles/hpsi_pb208_fp32.md.
+# states, one output): dram__bytes_read.sum + dram__bytes_write.sum of an
+# ncu capture of the same call (python -m hfb.microbench hpsi).
 HPSI_NCU_DRAM_BYTES = 433642496 + 388209920
 
 
