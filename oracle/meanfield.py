@@ -156,3 +156,63 @@ def skyrme(coulomb, dens, forces, grids, mf, tcoul=True):
     mf.upot, mf.bmass, mf.divaq, mf.v_pair = upot, bmass, divaq, vpair
     mf.aq, mf.spot, mf.wlspot, mf.dbmass = aq, spot, wlspot, dbmass
     return mf, coulomb
+
+
+def spectral_d1(n, d):
+    """Dense first-derivative matrix with the k = 0 and n/2 bins zeroed (the
+    first output of cderv00 / cderv02 as a matrix):
+    D[j, l] = -(2 kf / n) sum_{k=1}^{n/2-1} k sin(2 pi k (j - l) / n)."""
+    kf = 2.0 * np.pi / (n * d)
+    j = np.arange(n)
+    diff = j[:, None] - j[None, :]
+    k = np.arange(1, n // 2)[:, None, None]
+    return -(2.0 * kf / n) * np.sum(k * np.sin(2.0 * np.pi * k * diff / n), axis=0)
+
+
+def hpsi01_matrix_form(grids, mf, iq, weight, weightuv, pinn):
+    """hpsi01 (meanfield.py:41-159) in the form the single-precision
+    tensor-core kernel evaluates, in FP64: along each axis d,
+        out_d = L_d(D psi) + D(L_d psi - B D psi) + N_d,
+    with D the dense derivative above, L_d the pointwise current /
+    spin-orbit operator of axis d (the w of meanfield.py:77-84, 104-111,
+    133-140) and N_d = (pi/d)^2 mean_line(B) (-1)^j sum_l (-1)^l psi_l / n
+    the Nyquist bin cderv02 keeps (levels.py:314-315).  Equal to hpsi01 up
+    to rounding; a single 2-spinor (2, nx, ny, nz)."""
+    up, bm, aq, sp, wl, vp = (mf.upot[iq], mf.bmass[iq], mf.aq[iq], mf.spot[iq], mf.wlspot[iq], mf.v_pair[iq])
+    p0, p1 = pinn[0], pinn[1]
+    h = 0.5
+    o0 = up * p0 + (sp[0] - 1j * sp[1]) * p1 + sp[2] * p0
+    o1 = up * p1 + (sp[0] + 1j * sp[1]) * p0 - sp[2] * p1
+
+    def L(axis, a0, a1):
+        if axis == 0:
+            return (-1j * h * (aq[0] - wl[1]) * a0 - h * wl[2] * a1,
+                    -1j * h * (aq[0] + wl[1]) * a1 + h * wl[2] * a0)
+        if axis == 1:
+            return (-1j * h * (aq[1] + wl[0]) * a0 + 1j * h * wl[2] * a1,
+                    -1j * h * (aq[1] - wl[0]) * a1 + 1j * h * wl[2] * a0)
+        return (-1j * h * aq[2] * a0 + (h * wl[0] - 1j * h * wl[1]) * a1,
+                -1j * h * aq[2] * a1 + (-h * wl[0] - 1j * h * wl[1]) * a0)
+
+    for axis, d in enumerate((grids.dx, grids.dy, grids.dz)):
+        n = pinn.shape[1 + axis]
+        D = spectral_d1(n, d)
+        e0, e1 = apply_along(D, p0, axis), apply_along(D, p1, axis)
+        n0, n1 = L(axis, p0, p1)
+        l0, l1 = L(axis, e0, e1)
+        sign = (-1.0) ** np.arange(n)
+        shp = [1, 1, 1]
+        shp[axis] = n
+        sign = sign.reshape(shp)
+        bbar = np.mean(bm, axis=axis, keepdims=True)
+        nq = (np.pi / d) ** 2 / n
+        for c, (pc, ec, nc, lc) in enumerate(((p0, e0, n0, l0), (p1, e1, n1, l1))):
+            alt = np.sum(sign * pc, axis=axis, keepdims=True)
+            r = lc + apply_along(D, nc - bm * ec, axis) + nq * bbar * sign * alt
+            if c == 0:
+                o0 = o0 + r
+            else:
+                o1 = o1 + r
+    pout_mf = np.stack([o0, o1])
+    pout_del = pinn * vp
+    return weight * pout_mf - weightuv * pout_del, pout_mf, pout_del
