@@ -56,6 +56,14 @@ def test_ctx_create_rejects_bad_grids_without_gpu(lib):
 def test_null_arguments_are_rejected(lib):
     assert lib.hfb_hpsi(None, 0, None, 1, 1, None, None, None, None, None, None, None) == 1
     assert lib.hfb_pair(None, None, None) == 1
+    # observables, single-particle properties and constraints: a missing
+    # context or buffer is HFB_ERR_ARG before any device work
+    assert lib.hfb_observables(None, None, None, 8.0, 8.0, None, None) == 1
+    assert lib.hfb_sp_properties(None, 0, 4, None, None, None, None, None, None) == 1
+    assert lib.hfb_constraint_fields(None, 1, 16.0, 0.93, 6.0, 1.0, None, None) == 1
+    assert lib.hfb_constraint_moments(None, 1, None, None, None, None) == 1
+    assert lib.hfb_constraint_potential(None, 0, 1, None, None, None, None, None) == 1
+    assert lib.hfb_constraint_correct(None, 0, 1, 1, None, None, None, None, None, None) == 1
 
 
 def test_struct_layouts_match_c():
