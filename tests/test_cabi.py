@@ -165,3 +165,22 @@ def test_res_writer_matches_reference_text(tmp_path):
     for name, text in d["files"].items():
         with open(os.path.join(tmp_path, name), encoding="utf-8") as f:
             assert f.read() == text, name
+
+
+def test_observables_layout_matches_header():
+    """hfb.output's offsets into the hfb_observables output are the
+    HFB_OBS_* values of include/hfb.h and tile the HFB_NOBS doubles."""
+    from hfb import output
+    txt = open(HEADER).read()
+    enum = {k: int(v) for k, v in re.findall(r"HFB_OBS_(\w+)\s*=\s*(\d+)", txt)}
+    nobs = int(re.search(r"HFB_NOBS\s*=\s*(\d+)", txt).group(1))
+    names = {"pnr": "PNR", "cm": "CM", "pcm": "PCM", "rms": "RMS", "x2m": "X2M", "q20": "Q20", "q22": "Q22",
+             "pnrtot": "PNRTOT", "cmtot": "CMTOT", "rmstot": "RMSTOT", "x2mtot": "X2MTOT", "q20tot": "Q20TOT",
+             "q22tot": "Q22TOT", "q20T1": "Q20T1", "beta20tot": "BETA20", "beta22tot": "BETA22", "beta": "BETA",
+             "gamma": "GAMMA", "dipole_isovector": "DIPOLE", "qmat": "QMAT"}
+    assert nobs == output.HFB_NOBS
+    used = np.zeros(nobs, dtype=int)
+    for k, (off, shp) in output._OBS.items():
+        assert enum[names[k]] == off, k
+        used[off:off + int(np.prod(shp)) if shp else off + 1] += 1
+    assert np.all(used == 1)
