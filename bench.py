@@ -4,22 +4,33 @@ on one B200, plus the hpsi HBM roofline.
 Workload (default): Pb208, N = 126, Z = 82, SLy4 + volume-delta pairing
 (60 MeV soft window), 48^3 grid at dx = 0.8 fm, 140 + 96 two-spinor states,
 harmonic-oscillator start, doubled-grid Coulomb; synthetic inputs only (the
-reference ships no data).  One "step" is one self-consistent iteration.
+reference ships no data).  One "step" is one self-consistent iteration; the
+number of steps of a time-to-converge is set by the convergence test, not by
+``--steps``.
 
   1. W warm-up iterations (FP32 and FP64) on a throwaway state.
   2. FP64 run from the oscillator start until the geometric estimate of the
-     remaining energy change is below 0.005 keV: E_ref and the FP64
+     remaining energy change is below 1e-6 MeV: E_ref and the FP64
      time-to-converge (first iteration after which |E - E_ref| <= 1 keV).
+     A run that does not get there within the iteration cap reports no
+     E_ref and no value.
   3. Mixed run through the public API (hfb.static.statichf_mixed): FP32
-     bulk, FP64 refinement tail.  Its time-to-converge is ``value``; the
-     same run timed with the host->device copy of the initial states from
-     pinned memory and the device->host read of the results is ``e2e``.
-  4. hpsi on all 236 states, timed with CUDA events on the launching stream:
-     algorithmic bytes (read psi, write h psi, potentials once per isospin)
-     per launch / launch time = roofline.achieved.
-  5. CPU baseline: the NumPy oracle (restatement of the reference) timed on a
-     bounded sample of one iteration, scaled to the iterations the FP64 run
-     needed.
+     bulk, FP64 refinement tail.  Its time-to-converge (first FP64
+     iteration after which it stays within 1 keV of E_ref) is ``value``;
+     ``steps`` is that iteration count.  The same run timed with the
+     host->device copy of the initial states from pinned memory and the
+     device->host read of the results is ``e2e``.
+  4. hpsi on all 236 states, K = --steps timed launches with CUDA events on
+     the launching stream: algorithmic bytes (read psi, write h psi,
+     potentials once per isospin) per launch / launch time =
+     roofline.achieved.
+  5. CPU baseline: whole iterations of the NumPy oracle (restatement of the
+     reference) on all host cores, scaled to the FP64 iteration count this
+     run measured.
+
+``--impl reference`` times whole oracle iterations on all host cores (the
+reference's JAX cannot be installed here) and scales them to the FP64
+iteration count recorded for the workload.
 
 Multi-GPU: the path does not shard across GPUs in this build (replicas
 only): under torchrun every rank runs the same workload on its own GPU and
@@ -42,10 +53,13 @@ sys.path.insert(0, os.path.join(ROOT, "jax-hfbfft_b200"))
 METRIC = "Pb208 time-to-converge (ΔE≤1keV) mixed vs FP64 on B200; hpsi HBM GB/s vs peak"
 UNIT = "s"
 FALLBACK_HBM_GBS = 6650.0
-# SCF iterations the FP64 run of this algorithm needs to reach 1 keV on
-# Pb208 (measured with this bench's FP64 leg); scales the reference arm's
-# per-iteration CPU sample to a time-to-converge.
-PB208_FP64_ITERS = 675
+# FP64 iterations from the oscillator start to |E - E_limit| <= 1 keV, as
+# measured by this bench's FP64 leg on a B200 (same algorithm and step-size
+# rule as the oracle).  The reference arm, which cannot afford a converged
+# CPU run of the large workloads, scales its per-iteration time by these.
+FP64_ITERATIONS_TO_1KEV = {"Pb208": 661, "Cr48": 330, "O16": 230}
+# Upper bound on the seconds the reference arm spends on timed iterations.
+REFERENCE_ARM_BUDGET_S = 300.0
 # Both runs continue until the estimated remaining energy change is below
 # this (MeV): well past the 1 keV point that the time-to-converge reads, so
 # that the final states also carry converged single-particle energies for
@@ -55,6 +69,7 @@ STOP_MEV = 1e-6
 # states, one output): dram__bytes_read.sum + dram__bytes_write.sum of an
 # ncu capture of the same call (python -m hfb.microbench hpsi).
 HPSI_NCU_DRAM_BYTES = 433642496 + 388209920
+HPSI_KERNEL = "hpsi (ht_fields_kernel + hpsi_tc_kernel, tcgen05), FP32, 236 states"
 
 
 def _peaks():
@@ -150,7 +165,10 @@ def converged_index(E, e_ref, tol, allowed):
 
 
 def fp64_run(case_name, maxiter):
-    """Plain FP64 run with per-iteration CUDA events."""
+    """Plain FP64 run with per-iteration CUDA events, until the estimated
+    remaining energy change is below STOP_MEV.  ``converged`` is False when
+    the cap was reached first; e_ref is then None (an energy extrapolated
+    from an unconverged trajectory is not a reference)."""
     import torch
     from hfb import static
     st = _state(case_name, torch.complex128)
@@ -160,6 +178,7 @@ def fp64_run(case_name, maxiter):
     ev0.record()
     static.prepare(**S)
     evs, E = [], []
+    converged = False
     for i in range(1, maxiter + 1):
         static.iterate(i, **S)
         e = torch.cuda.Event(enable_timing=True)
@@ -168,11 +187,13 @@ def fp64_run(case_name, maxiter):
         E.append(st["energies"].ehf)
         rem = static.remaining_change(E)
         if i > 60 and rem is not None and abs(rem) < STOP_MEV:
+            converged = True
             break
     torch.cuda.synchronize()
     t = [ev0.elapsed_time(e) / 1e3 for e in evs]
-    rem = static.remaining_change(E) or 0.0
-    return dict(E=E, t=t, e_ref=E[-1] + rem, iters=len(E), state=st)
+    rem = static.remaining_change(E)
+    e_ref = E[-1] + rem if converged else None
+    return dict(E=E, t=t, e_ref=e_ref, converged=converged, iters=len(E), state=st)
 
 
 def mixed_e2e_run(case_name, maxiter, switch_mev=5e-4):
@@ -191,14 +212,17 @@ def mixed_e2e_run(case_name, maxiter, switch_mev=5e-4):
     e_d2h0 = torch.cuda.Event(enable_timing=True)
     e_d2h1 = torch.cuda.Event(enable_timing=True)
 
+    from hfb._lib import launch_count
+    L = []
+
     def on_it(i, e, prec):
         ev = torch.cuda.Event(enable_timing=True)
         ev.record()
         evs.append(ev)
         E.append(e)
         P.append(prec)
+        L.append(launch_count())
 
-    from hfb._lib import launch_count
     n0 = launch_count()
     torch.cuda.synchronize()
     e_h2d0.record()
@@ -215,13 +239,14 @@ def mixed_e2e_run(case_name, maxiter, switch_mev=5e-4):
     n1 = launch_count()
     bytes_out = out_rho.numel() * 8 + out_spe.numel() * 8 + 8
     t = [e_h2d1.elapsed_time(e) / 1e3 for e in evs]
-    return dict(E=E, t=t, P=P, switch=sw, iters=len(E), state=st, launches=n1 - n0,
+    return dict(E=E, t=t, P=P, switch=sw, iters=len(E), state=st, launches=n1 - n0, launches_at=[x - n0 for x in L],
                 h2d_s=e_h2d0.elapsed_time(e_h2d1) / 1e3, d2h_s=e_d2h0.elapsed_time(e_d2h1) / 1e3,
                 bytes_in=bytes_in, bytes_out=bytes_out)
 
 
-def hpsi_roofline(st, reps=20):
-    """Time hpsi over all states in FP32 on the converged state."""
+def hpsi_roofline(st, reps=20, warm=3):
+    """Time ``reps`` back-to-back hpsi launches over all states in FP32 on
+    the converged state (the states, 0.42 GB, are larger than L2)."""
     import torch
     from hfb._lib import call, ptr, stream_ptr, prec_of
     lv, mf, g = st["levels"], st["meanfield"], st["grids"]
@@ -237,7 +262,7 @@ def hpsi_roofline(st, reps=20):
         call("hfb_hpsi", g.ctx.handle, prec_of(psi), ptr(mf.pot), ns, nn, ptr(psi), ptr(wt), ptr(wu), None, ptr(out),
              None, stream_ptr())
 
-    for _ in range(3):
+    for _ in range(max(warm, 3)):
         once()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -253,74 +278,61 @@ def hpsi_roofline(st, reps=20):
     return t, bytes_alg
 
 
-def cpu_sample(case_name, nsub=16):
-    """One oracle (NumPy, FP64) self-consistent iteration of the workload on
-    the host: the per-state work (two hpsi, the preconditioner, the densities
-    and the kinetic energy) on ``nsub`` states scaled to all states; the
-    diagonalisation step, BCS, potentials, Coulomb and energies in full.
-    Returns (seconds per iteration, description)."""
+def oracle_iterations(case_name, n_iter, warm=1, budget_s=None, threads=None):
+    """Whole self-consistent iterations of the NumPy oracle (FP64, the
+    restatement of the reference's static.py:1755-1882 loop body) on the
+    host, the per-state work spread over ``threads`` host threads (default:
+    every core).  ``warm`` untimed iterations follow the set-up; then up to
+    ``n_iter`` timed ones, fewer if the next would pass ``budget_s``.
+    Returns (list of per-iteration seconds, threads, description)."""
     sys.path.insert(0, ROOT)
-    import numpy as np
     from hfb import config
-    from oracle import model, static as ost, meanfield as omf, densities as od, spectral, coulomb as oc
-    from oracle import energies as oe, pairs as op
-    case = config.case_dict(case_name)
-    g = model.init_grids(**case["grid"])
-    f = model.init_forces(**case["force"])
-    lvc = case["levels"]
-    lv = model.init_levels(g, lvc["nneut"], lvc["nprot"], tuple(lvc["npsi"]))
-    f, st = ost.init_static(f, lv, **case["static"])
-    lv = ost.harmosc(g, lv, st)
-    rs = ost.RunState(params=dict(mprint=1), forces=f, grids=g, levels=lv, mf=omf.init_meanfield(g),
-                      dens=od.init_densities(g), coulomb=oc.init_coulomb(g), st=st, en=oe.Energies(),
-                      pairs=op.Pairs())
-    sub = lv.psi[:nsub]
-    w = np.ones(nsub)
-    t0 = time.perf_counter()
-    for _ in range(2):
-        omf.hpsi01(g, rs.mf, 0, w, 0 * w, sub)
-    for k in range(nsub):
-        spectral.laplace(g, f.h2ma, 1.0, 0.0, sub[k], 0.0, 100.0)
-    od.state_contributions(w, w, sub, g.d)
-    np.fft.fftn(sub, axes=(2, 3, 4))
-    np.fft.ifftn(sub, axes=(2, 3, 4))
-    t_state = (time.perf_counter() - t0) / nsub
-    t1 = time.perf_counter()
-    rs.en, rs.levels, rs.st = ost.diagstep(rs.en, f, g, rs.levels, rs.st, True, True)
-    rs.dens.rho[:] = 0.08
-    rs.mf, rs.coulomb = omf.skyrme(rs.coulomb, rs.dens, f, g, rs.mf)
-    oe.integ_energy(rs.coulomb, rs.dens, rs.en, f, g, rs.levels, rs.pairs)
-    t_global = time.perf_counter() - t1
-    per_it = lv.nstmax * t_state + t_global
-    desc = (f"one {case_name} iteration of the NumPy oracle: per-state work timed on {nsub} of {lv.nstmax} states "
-            f"and scaled; diagonalisation, potentials, Coulomb and energies in full")
-    return per_it, desc
+    from oracle import static as ost, pool
+    threads = threads or os.cpu_count() or 1
+    pool.set_workers(threads)
+    rs = ost.build(config.case_dict(case_name))
+    ost.prepare(rs)
+    i = 0
+    for _ in range(warm):
+        i += 1
+        ost.iterate(rs, i)
+    times = []
+    total = 0.0
+    for _ in range(max(n_iter, 1)):
+        if times and budget_s is not None and total + statistics.mean(times) > budget_s:
+            break
+        i += 1
+        t0 = time.perf_counter()
+        ost.iterate(rs, i)
+        times.append(time.perf_counter() - t0)
+        total += times[-1]
+    pool.set_workers(1)
+    desc = (f"{len(times)} whole {case_name} iterations (after set-up and {warm} untimed) of the NumPy FP64 oracle, "
+            f"per-state work on {threads} host threads; restatement of the reference, not its JAX code")
+    return times, threads, desc
 
 
 def reference_arm(args, rank, world):
-    """The reference's CPU path on the host cores: the oracle port (JAX is not
-    installable here).  Each step is one bounded sample (cpu_sample); the
-    value scales the median per-iteration time to the FP64 iteration count."""
+    """The reference's CPU path on the host cores.  JAX is not installable
+    here, so this is the oracle port: whole iterations, timed one per step,
+    scaled to the FP64 iteration count recorded for the workload."""
     if rank != 0:
         return None
-    k = max(args.steps, 1) if args.steps > 0 else 1
-    nsub = 16 if k + args.warmup <= 6 else 4
-    for _ in range(min(args.warmup, 1)):
-        cpu_sample(args.workload, nsub=2)
-    samples = []
-    desc = ""
-    for _ in range(k):
-        s, desc = cpu_sample(args.workload, nsub=nsub)
-        samples.append(s)
-    per_it = statistics.median(samples)
-    value = per_it * PB208_FP64_ITERS
-    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=len(samples), warmup=min(args.warmup, 1),
-                ms_per_step=per_it * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None, dtype="f64",
-                data="synthetic", impl="reference",
+    times, threads, desc = oracle_iterations(args.workload, max(args.steps, 1), warm=min(max(args.warmup, 1), 2),
+                                             budget_s=REFERENCE_ARM_BUDGET_S)
+    per_it = statistics.median(times)
+    iters = FP64_ITERATIONS_TO_1KEV.get(args.workload)
+    value = per_it * iters if iters else None
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=len(times),
+                warmup=min(max(args.warmup, 1), 2), ms_per_step=per_it * 1e3, higher_is_better=False,
+                scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
                 config=dict(workload=f"{args.workload} HF-BCS (the bench workload), FP64 NumPy oracle on host cores",
-                            iterations_assumed=PB208_FP64_ITERS),
-                cpu_baseline=dict(value=value, unit=UNIT, cores=os.cpu_count(), kind="port",
-                                  sample=desc + f"; x {PB208_FP64_ITERS} iterations"),
+                            step="one whole self-consistent iteration of the oracle",
+                            fp64_iterations_to_1kev=iters,
+                            iterations_source="FP64 GPU run of the same algorithm (bench FP64 leg)",
+                            seconds_timed=sum(times)),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=threads, kind="port",
+                                  sample=desc + f"; median iteration x {iters} iterations"),
                 e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     return line
 
@@ -328,11 +340,14 @@ def reference_arm(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=0, help="max SCF iterations per run (0 = until converged)")
+    ap.add_argument("--steps", type=int, default=20,
+                    help="timed hpsi launches of the roofline (reference arm: timed oracle iterations); the "
+                         "self-consistent runs always go to convergence")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--workload", default="Pb208")
     ap.add_argument("--tol-kev", type=float, default=1.0)
+    ap.add_argument("--max-iter", type=int, default=4000, help="iteration cap of each self-consistent run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--switch-mev", type=float, default=5e-4,
                     help="mixed run: estimated remaining change (MeV) at which FP32 hands over to FP64")
@@ -352,36 +367,38 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    maxiter = args.steps if args.steps > 0 else 4000
     tol = args.tol_kev * 1e-3
-    warmup(args.workload, max(args.warmup, 3))
-    # FP64 reference run
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    r64 = fp64_run(args.workload, maxiter)
-    e_ref = r64["e_ref"]
-    i64 = converged_index(r64["E"], e_ref, tol, [True] * len(r64["E"]))
-    t64 = r64["t"][i64] if i64 is not None else None
-    # mixed run (the timed region of the headline number)
+    W = max(args.warmup, 3)
+    warmup(args.workload, W)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        rm = mixed_e2e_run(args.workload, maxiter, args.switch_mev)
-    torch.cuda.synchronize()
+        # FP64 run: the reference energy and the denominator of the speed-up
+        r64 = fp64_run(args.workload, args.max_iter)
+        e_ref = r64["e_ref"]
+        i64 = converged_index(r64["E"], e_ref, tol, [True] * len(r64["E"])) if e_ref is not None else None
+        t64 = r64["t"][i64] if i64 is not None else None
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        # mixed run through the public driver (the headline's timed region)
+        rm = mixed_e2e_run(args.workload, args.max_iter, args.switch_mev)
+        torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    im = converged_index(rm["E"], e_ref, tol, [p == "f64" for p in rm["P"]])
-    tm = rm["t"][im] if im is not None else None
-    value = tm
-    if dist and value is not None:
-        v = torch.tensor([value, t64 or 0.0], device="cuda", dtype=torch.float64)
+    im = converged_index(rm["E"], e_ref, tol, [p == "f64" for p in rm["P"]]) if e_ref is not None else None
+    value = rm["t"][im] if im is not None else None
+    e2e = None if value is None else rm["h2d_s"] + value + rm["d2h_s"]
+    if dist:
+        v = torch.tensor([value or 0.0, t64 or 0.0, e2e or 0.0], device="cuda", dtype=torch.float64)
         dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        value, t64 = float(v[0]), float(v[1])
-    e2e = None if tm is None else rm["h2d_s"] + tm + rm["d2h_s"]
-    # hpsi roofline
-    t_h, b_h = hpsi_roofline(rm["state"])
+        value = float(v[0]) if value is not None else None
+        t64 = float(v[1]) if t64 is not None else None
+        e2e = float(v[2]) if e2e is not None else None
+    steps = (im + 1) if im is not None else None
+    # hpsi roofline: K timed launches
+    t_h, b_h = hpsi_roofline(rm["state"], reps=max(args.steps, 1), warm=W)
     peak, peak_kind = _peaks()
     achieved = b_h / t_h / 1e9
     from hfb.output import rms_radii
@@ -405,32 +422,40 @@ def main():
     occ = w_64 > 1e-2
     d_spe_occ = float(np.max(np.abs(e_m - e_64)[occ])) if occ.any() else None
     line = dict(
-        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=im + 1 if im is not None else rm["iters"],
-        warmup=max(args.warmup, 3), ms_per_step=(value / (im + 1) * 1e3) if value else None, higher_is_better=False,
+        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=steps, warmup=W,
+        ms_per_step=(value / steps * 1e3) if value else None, higher_is_better=False,
         scaling="weak", vs_baseline=None, dtype="f32+f64", data="synthetic",
         config=dict(workload=f"{args.workload} HF-BCS: SLy4 + volume-delta pairing, 48^3 grid dx 0.8 fm, "
                              "140+96 2-spinor states, HO start, 96^3 Coulomb grid",
+                    step="one self-consistent iteration; steps = mixed iterations to |E - E_ref| <= tol",
                     parallelism="replicas" if world > 1 else "single GPU",
                     l2="inputs larger than L2 (states 0.5-0.8 GB)", tolerance_kev=args.tol_kev,
-                    fp64_time_to_converge_s=t64, fp64_iterations=(i64 + 1) if i64 is not None else None,
+                    fp64_converged=r64["converged"], fp64_time_to_converge_s=t64,
+                    fp64_iterations=(i64 + 1) if i64 is not None else None,
+                    fp64_iterations_run=r64["iters"],
                     speedup_mixed_vs_fp64=(t64 / value) if (t64 and value) else None,
-                    mixed_iterations=(im + 1) if im is not None else None, mixed_switch_iteration=rm["switch"],
+                    mixed_iterations=steps, mixed_iterations_run=rm["iters"],
+                    mixed_switch_iteration=rm["switch"],
                     e_ref_mev=e_ref, e_mixed_final_mev=rm["E"][-1],
-                    de_final_kev=abs(rm["E"][-1] - e_ref) * 1e3, rms_proton_fm=rms[1],
+                    de_final_kev=(abs(rm["E"][-1] - e_ref) * 1e3) if e_ref is not None else None,
+                    rms_proton_fm=rms[1],
                     d_rms_proton_fm_vs_fp64=abs(rms[1] - rms64[1]), d_sp_energy_max_mev_vs_fp64=d_spe,
                     d_sp_energy_occupied_max_mev_vs_fp64=d_spe_occ,
                     fp64_ms_per_iteration=(r64["t"][-1] / r64["iters"] * 1e3)),
         roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
-                      traffic=HPSI_NCU_DRAM_BYTES, kernel="hpsi (ht_fields_kernel + hpsi_tc_kernel, tcgen05), FP32, 236 states",
-                      launch_ms=t_h * 1e3, bytes_per_launch=b_h, peak_kind=peak_kind),
-        e2e=dict(value=e2e, unit=UNIT, h2d_bytes_per_step=rm["bytes_in"] / max(rm["iters"], 1),
-                 d2h_bytes_per_step=rm["bytes_out"] / max(rm["iters"], 1)),
-        gpu_launches=rm["launches"], clocks=clk.summary())
+                      traffic=HPSI_NCU_DRAM_BYTES, kernel=HPSI_KERNEL, launch_ms=t_h * 1e3, bytes_per_launch=b_h,
+                      peak_kind=peak_kind, launches_timed=max(args.steps, 1)),
+        e2e=dict(value=e2e, unit=UNIT, h2d_bytes_per_step=rm["bytes_in"] / steps if steps else None,
+                 d2h_bytes_per_step=rm["bytes_out"] / steps if steps else None),
+        gpu_launches=rm["launches_at"][im] if steps else rm["launches"], clocks=clk.summary())
+    if e_ref is None:
+        line["error"] = f"FP64 run not converged within {args.max_iter} iterations: no reference energy"
     if rank == 0 and world == 1 and not args.no_cpu:
-        per_it, desc = cpu_sample(args.workload)
-        iters = (i64 + 1) if i64 is not None else PB208_FP64_ITERS
-        line["cpu_baseline"] = dict(value=per_it * iters, unit=UNIT, cores=os.cpu_count(), kind="port",
-                                    sample=desc + f"; x {iters} iterations")
+        times, threads, desc = oracle_iterations(args.workload, 2, warm=0, budget_s=30.0)
+        per_it = statistics.median(times)
+        iters = (i64 + 1) if i64 is not None else None
+        line["cpu_baseline"] = dict(value=per_it * iters if iters else None, unit=UNIT, cores=threads, kind="port",
+                                    sample=desc + f"; median iteration x {iters} FP64 iterations of this run")
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -108,17 +108,20 @@ int hfb_skyrme(hfb_ctx_t ctx, const hfb_force* f, int tcoul, const double* rho, 
 /* poisson (coulomb.py:54-75): wcoul[nx][ny][nz] from the proton density. */
 int hfb_poisson(hfb_ctx_t ctx, const double* rho_p, double* wcoul, void* stream);
 /* Same result as hfb_poisson without allocating device memory during the
- * call (no counterpart in the reference): for callers that may not allocate
- * at call time -- work being recorded into a CUDA graph, applications whose
- * device memory belongs to their own pool allocator, latency-critical loops.
- * The work buffer is a fixed 4 MiB array inside the library (64^3 complex
- * doubles), so the doubled Coulomb grid is limited to 64^3: grids up to 32^3
- * (non-periodic); larger grids return HFB_ERR_UNSUPPORTED_GRID.  The first
- * call on each device looks up the array's device address, so make that
- * first call before any stream capture.  All calls share the one buffer (it
- * keeps the last call's contents; each call rewrites all of it, padding
- * zeros included): calls that overlap on the GPU -- concurrent streams,
- * host threads -- race and must be serialised by the caller. */
+ * call (no counterpart in the reference), for callers that cannot let the
+ * library allocate: applications whose device memory is entirely owned by
+ * their own pool allocator, and latency-critical loops where an allocation
+ * and the synchronisation it implies would stall.  The work buffer is a
+ * fixed 4 MiB array inside the library (64^3 complex doubles), so the
+ * Coulomb grid n2 must be at most 64^3: n <= 32 for a non-periodic grid
+ * (n2 = 2n); every periodic grid a context accepts (n2 = n <= 48) fits.
+ * Larger Coulomb grids return HFB_ERR_UNSUPPORTED_GRID.  Call it with the context's device current
+ * (HFB_ERR_ARG otherwise).  The first call on each device looks up the
+ * array's device address, so make that first call before any stream
+ * capture.  All calls share the one buffer (it keeps the last call's
+ * contents; each call rewrites all of it, padding zeros included): calls
+ * that overlap on the GPU -- concurrent streams, host threads -- race and
+ * must be serialised by the caller. */
 int hfb_poisson_noalloc(hfb_ctx_t ctx, const double* rho_p, double* wcoul, void* stream);
 
 /* ---- densities.py / inout.py ------------------------------------------- */

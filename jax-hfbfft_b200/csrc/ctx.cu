@@ -83,6 +83,11 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
   c->wxyz = dx * dy * dz;
   c->periodic = periodic ? 1 : 0;
   c->nstmax = nstmax;
+  if (cudaGetDevice(&c->device) != cudaSuccess) {
+    cudaGetLastError();
+    free(c);
+    return HFB_ERR_CUDA;
+  }
   c->n2 = periodic ? nx : 2 * nx;
   {
     const char* e = getenv("HFB_NO_TCGEN05");

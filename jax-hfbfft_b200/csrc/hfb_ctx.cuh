@@ -10,6 +10,7 @@ struct hfb_ctx_s {
   double wxyz;
   int periodic;
   int nstmax;
+  int device;            // CUDA device current when the context was created
   int n2;                // Coulomb grid size (2n, or n when periodic)
   double* der1[3];       // dense spectral derivative matrices (grids.py:36-61)
   double* der2[3];

@@ -317,11 +317,11 @@ __global__ void pois_store_kernel(const double2* a, int n, int n2, double scale,
   w[i] = scale * a[((size_t)x * n2 + y) * n2 + z].x;
 }
 
-int poisson_launch(hfb_ctx_s* c, const double* rho_p, double* wcoul, cudaStream_t st) {
+// The doubled-grid solve on the work buffer ``a`` (n2^3 complex doubles;
+// every element is rewritten, so it may hold anything on entry).
+static int poisson_solve(const hfb_ctx_s* c, const double* rho_p, double* wcoul, double2* a, cudaStream_t st) {
   const int n = c->n, n2 = c->n2;
   const size_t tot = (size_t)n2 * n2 * n2;
-  double2* a = (double2*)scratch(c, hfb_ctx_s::S_POIS, tot * sizeof(double2));
-  if (!a) return HFB_ERR_ALLOC;
   pois_load_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(a, n, n2, rho_p);
   HFB_CHECK_LAUNCH();
   const bool pruned = !c->periodic;
@@ -344,6 +344,13 @@ int poisson_launch(hfb_ctx_s* c, const double* rho_p, double* wcoul, cudaStream_
   pois_store_kernel<<<(unsigned)((t3 + 255) / 256), 256, 0, st>>>(a, n, n2, 1.0 / (double)tot, wcoul);
   HFB_CHECK_LAUNCH();
   return HFB_OK;
+}
+
+int poisson_launch(hfb_ctx_s* c, const double* rho_p, double* wcoul, cudaStream_t st) {
+  const size_t tot = (size_t)c->n2 * c->n2 * c->n2;
+  double2* a = (double2*)scratch(c, hfb_ctx_s::S_POIS, tot * sizeof(double2));
+  if (!a) return HFB_ERR_ALLOC;
+  return poisson_solve(c, rho_p, wcoul, a, st);
 }
 
 // ----------------------------------------------------- potential assembly --
@@ -487,19 +494,19 @@ extern "C" int hfb_skyrme(hfb_ctx_t ctx, const hfb_force* f, int tcoul, const do
 }
 
 // --------------------------------------------- Poisson without allocation --
-// A second entry point for the Coulomb solve for callers that must not
-// allocate device memory when they call the library: code that is being
-// recorded into a CUDA graph (an allocation inside stream capture is not
-// part of the graph and breaks the capture), applications whose device
-// memory is entirely owned by their own pool allocator, and latency-critical
-// loops where an allocation and its implicit synchronisation would stall.
+// A second entry point for the Coulomb solve, for callers that cannot let
+// the library allocate device memory when they call it: applications whose
+// device memory is entirely owned by their own pool allocator (a cudaMalloc
+// behind its back can fail or fragment the pool), and latency-critical loops
+// where an allocation, with the synchronisation it implies, would stall.
 // Its work buffer is a fixed array in the library's device image instead of
 // the context's growable scratch arena.
 namespace hfb {
 
-// Doubled-grid work buffer: 64^3 complex doubles (4 MiB), i.e. grids up to
-// 32^3 (non-periodic) or 64^3 (periodic).  Every GPU that loads the library
-// holds it until the process exits.
+// Doubled-grid work buffer: 64^3 complex doubles (4 MiB).  The Coulomb grid
+// n2 (2n non-periodic, n periodic) must be at most 64: n <= 32 for a
+// non-periodic grid; every periodic grid a context accepts (n <= 48) fits.
+// Every GPU that loads the library holds it until the process exits.
 constexpr int kNoAllocN2 = 64;
 static __device__ __align__(256) double2 g_poisson_noalloc[(size_t)kNoAllocN2 * kNoAllocN2 * kNoAllocN2];
 
@@ -509,9 +516,8 @@ static __device__ __align__(256) double2 g_poisson_noalloc[(size_t)kNoAllocN2 * 
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[64] = {nullptr};
 
-static int noalloc_buffer(double2** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HFB_ERR_CUDA;
+static int noalloc_buffer(int dev, double2** out) {
+  if (dev < 0 || dev >= 64) return HFB_ERR_CUDA;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   if (!g_noalloc_addr[dev]) {
     void* p = nullptr;
@@ -530,34 +536,19 @@ static int noalloc_buffer(double2** out) {
 extern "C" int hfb_poisson_noalloc(hfb_ctx_t ctx, const double* rho_p, double* wcoul, void* stream) {
   using namespace hfb;
   if (!ctx || !rho_p || !wcoul) return HFB_ERR_ARG;
-  const int n = ctx->n, n2 = ctx->n2;
-  if (n2 > kNoAllocN2) return HFB_ERR_UNSUPPORTED_GRID;   // work buffer too small for this grid
+  if (ctx->n2 > kNoAllocN2) return HFB_ERR_UNSUPPORTED_GRID;   // work buffer too small for this grid
+  // the buffer is looked up on the current device; the context's Green's
+  // function lives on the device it was created on: they must be the same
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return HFB_ERR_CUDA;
+  }
+  if (dev != ctx->device) return HFB_ERR_ARG;
   double2* a = nullptr;
-  int r = noalloc_buffer(&a);
+  const int r = noalloc_buffer(dev, &a);
   if (r) return r;
-  cudaStream_t st = as_stream(stream);
-  const size_t tot = (size_t)n2 * n2 * n2;
-  // the load writes every element of the n2^3 region: the zero padding
-  // outside the density is re-established on each call
-  pois_load_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(a, n, n2, rho_p);
-  HFB_CHECK_LAUNCH();
-  const bool pruned = !ctx->periodic;
-  r = dispatch_n2(n2, [&](auto nn) -> int {
-    constexpr int N2 = decltype(nn)::value;
-    return coul_fft3<N2, -1>(a, n, pruned, st);
-  });
-  if (r) return r;
-  const double e2 = 1.4399784085965135;
-  const double fac = ctx->periodic ? 4.0 * kPi * e2 : e2 * ctx->wxyz;
-  pois_mul_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(a, ctx->coul_q, tot, fac, ctx->periodic);
-  HFB_CHECK_LAUNCH();
-  r = dispatch_n2(n2, [&](auto nn) -> int {
-    constexpr int N2 = decltype(nn)::value;
-    return coul_fft3<N2, +1>(a, n, pruned, st);
-  });
-  if (r) return r;
-  const size_t t3 = (size_t)n * n * n;
-  pois_store_kernel<<<(unsigned)((t3 + 255) / 256), 256, 0, st>>>(a, n, n2, 1.0 / (double)tot, wcoul);
-  HFB_CHECK_LAUNCH();
-  return HFB_OK;
+  // the solve rewrites every element of the n2^3 region, padding zeros
+  // included, so nothing left by an earlier call leaks into this one
+  return poisson_solve(ctx, rho_p, wcoul, a, as_stream(stream));
 }

@@ -6,6 +6,7 @@ unused helper at densities.py:33-175 is not restated).
 from dataclasses import dataclass
 import numpy as np
 
+from . import pool
 from .spectral import cderv00
 
 
@@ -66,10 +67,18 @@ def add_density(dens, grids, levels):
     weightuv = levels.wguv * levels.pairwg * levels.wstates
     out = {k: [] for k in ("rho", "chi", "tau", "current", "sdens", "sodens")}
     for iq in range(2):
-        sl = levels.block(iq)
-        r = state_contributions(weight[sl], weightuv[sl], levels.psi[sl], grids.d)
-        for k, v in zip(out, r):
-            out[k].append(v.sum(axis=0))
+        b = levels.block(iq)
+
+        def part(sl):
+            r = state_contributions(weight[sl], weightuv[sl], levels.psi[sl], grids.d)
+            return [v.sum(axis=0) for v in r]
+
+        parts = pool.pmap(part, pool.chunks(b.start, b.stop))
+        for j, k in enumerate(out):
+            acc = parts[0][j]
+            for p in parts[1:]:
+                acc = acc + p[j]
+            out[k].append(acc)
     for k in out:
         setattr(dens, k, np.stack(out[k]))
     return dens

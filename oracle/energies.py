@@ -5,6 +5,7 @@ Follows reference energies.py:8-372, inout.py:64-150 and output.py:177-246.
 from dataclasses import dataclass, field
 import numpy as np
 
+from . import pool
 from .model import apply_along
 from .spectral import cderv01, k2_total
 
@@ -123,30 +124,38 @@ def sp_properties(forces, grids, levels, cmtot=(0.0, 0.0, 0.0)):
     xx = (grids.x - cmtot[0])[None, :, None, None]
     yy = (grids.y - cmtot[1])[None, None, :, None]
     zz = (grids.z - cmtot[2])[None, None, None, :]
-    lap = np.fft.ifftn(np.fft.fftn(psi, axes=(2, 3, 4)) * k2_total(grids)[None, None], axes=(2, 3, 4))
-    kin_raw = -np.sum((np.conj(psi) * lap).real, axis=(1, 2, 3, 4))
+    k2 = k2_total(grids)[None, None]
     h2m = np.where(levels.isospin == 0, forces.h2m[0], forces.h2m[1])
-    levels.sp_kinetic = w * h2m * kin_raw
+    kin = np.zeros(levels.nstmax)
     orb = np.zeros((levels.nstmax, 3))
     spin = np.zeros((levels.nstmax, 3))
     par = np.zeros(levels.nstmax)
-    for i in range(levels.nstmax):
-        pst = psi[i]
-        px, _ = cderv01(grids.dx, pst, 1)
-        py, _ = cderv01(grids.dy, pst, 2)
-        pz, _ = cderv01(grids.dz, pst, 3)
-        re, im = pst.real, pst.imag
-        orb[i] = w * np.array([
-            np.sum(re * (yy[0] * pz.imag - zz[0] * py.imag) + im * (zz[0] * py.real - yy[0] * pz.real)),
-            np.sum(re * (zz[0] * px.imag - xx[0] * pz.imag) + im * (xx[0] * pz.real - zz[0] * px.real)),
-            np.sum(re * (xx[0] * py.imag - yy[0] * px.imag) + im * (yy[0] * px.real - xx[0] * py.real))])
-        a, b = pst[0], pst[1]
-        spin[i] = w * 0.5 * np.array([
-            np.sum((np.conj(a) * b).real + (np.conj(b) * a).real),
-            np.sum((np.conj(a) * b * (-1j)).real + (np.conj(b) * a * 1j).real),
-            np.sum((np.conj(a) * a).real - (np.conj(b) * b).real)])
-        fl = pst[:, ::-1, ::-1, ::-1]
-        par[i] = w * np.sum(re * fl.real + im * fl.imag)
+
+    def part(sl):
+        # states of ``sl``: writes disjoint entries
+        ps = psi[sl]
+        lap = np.fft.ifftn(np.fft.fftn(ps, axes=(2, 3, 4)) * k2, axes=(2, 3, 4))
+        kin[sl] = w * h2m[sl] * -np.sum((np.conj(ps) * lap).real, axis=(1, 2, 3, 4))
+        for i in range(sl.start, sl.stop):
+            pst = psi[i]
+            px, _ = cderv01(grids.dx, pst, 1)
+            py, _ = cderv01(grids.dy, pst, 2)
+            pz, _ = cderv01(grids.dz, pst, 3)
+            re, im = pst.real, pst.imag
+            orb[i] = w * np.array([
+                np.sum(re * (yy[0] * pz.imag - zz[0] * py.imag) + im * (zz[0] * py.real - yy[0] * pz.real)),
+                np.sum(re * (zz[0] * px.imag - xx[0] * pz.imag) + im * (xx[0] * pz.real - zz[0] * px.real)),
+                np.sum(re * (xx[0] * py.imag - yy[0] * px.imag) + im * (yy[0] * px.real - xx[0] * py.real))])
+            a, b = pst[0], pst[1]
+            spin[i] = w * 0.5 * np.array([
+                np.sum((np.conj(a) * b).real + (np.conj(b) * a).real),
+                np.sum((np.conj(a) * b * (-1j)).real + (np.conj(b) * a * 1j).real),
+                np.sum((np.conj(a) * a).real - (np.conj(b) * b).real)])
+            fl = pst[:, ::-1, ::-1, ::-1]
+            par[i] = w * np.sum(re * fl.real + im * fl.imag)
+
+    pool.pmap(part, pool.chunks(0, levels.nstmax))
+    levels.sp_kinetic = kin
     levels.sp_orbital, levels.sp_spin, levels.sp_parity = orb, spin, par
     return levels
 

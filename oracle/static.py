@@ -7,6 +7,7 @@ Follows reference static.py:21-738 and the loop body of
 from dataclasses import dataclass, field
 import numpy as np
 
+from . import pool
 from .spectral import laplace
 from .meanfield import hpsi01, skyrme
 from .densities import add_density
@@ -134,8 +135,8 @@ def grstep(forces, grids, levels, mf, iteration, st, mprint=1):
     ef1 = levels.sp_efluct1.copy()
     ef2 = levels.sp_efluct2.copy()
     denerg = np.zeros(nst)
-    for iq in range(2):
-        sl = levels.block(iq)
+    def block(iq, sl):
+        # the states of ``sl`` (all of isospin iq); writes disjoint slices
         ps1, pmf, _ = hpsi01(grids, mf, iq, wt[sl], wu[sl], levels.psi[sl])
         vmax = np.max(mf.v_pair[iq])
         for loc, k in enumerate(range(sl.start, sl.stop)):
@@ -164,6 +165,12 @@ def grstep(forces, grids, levels, mf, iteration, st, mprint=1):
         _, hm, dl = hpsi01(grids, mf, iq, wt[sl], wu[sl], new_psi[sl])         # (194-208)
         hmfpsi[sl] = hm
         delpsi[sl] = dl
+
+    jobs = []
+    for iq in range(2):
+        b = levels.block(iq)
+        jobs += [(iq, c) for c in pool.chunks(b.start, b.stop)]
+    pool.pmap(lambda j: block(*j), jobs)
     levels.psi, levels.hampsi, levels.hmfpsi, levels.delpsi = new_psi, hampsi, hmfpsi, delpsi
     levels.sp_energy = spe_new
     levels.sp_efluct1, levels.sp_efluct2 = ef1, ef2

@@ -8,7 +8,7 @@ docstring of ``jaxshim/jax/__init__.py`` for the semantics restated).
 Run from the repository root, in the build container only (it reads the
 reference checkout)::
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <path of the reference checkout>
 
 Outputs (committed): ``tests/golden/unit_n8.npz`` (per-function vectors on an
 8^3 grid with seeded random inputs), ``tests/golden/run_<case>.npz``
@@ -376,7 +376,7 @@ def constraint_vectors(m, ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="path of the unmodified reference checkout")
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
     m = _import_reference(a.ref)

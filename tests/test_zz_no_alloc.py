@@ -22,10 +22,13 @@ def _solve(lib_name, g, rho):
     return w.cpu().numpy()
 
 
-@pytest.mark.parametrize("n,d", [(16, 1.0), (32, 0.8)])
-def test_poisson_noalloc_matches_allocating_solve_twice(n, d):
+@pytest.mark.parametrize("n,d,periodic", [(16, 1.0, False), (32, 0.8, False), (32, 0.8, True), (48, 0.8, True)])
+def test_poisson_noalloc_matches_allocating_solve_twice(n, d, periodic):
+    """Non-periodic grids (doubled Coulomb grid 2n, pruned padding) and
+    periodic ones (Coulomb grid n, 1/k^2 Green's function): the periodic
+    48^3 grid fills 48^3 of the 64^3 buffer."""
     import hfb
-    g = hfb.grids.init_grids(hfb.params.init_params(), nx=n, ny=n, nz=n, dx=d, dy=d, dz=d)
+    g = hfb.grids.init_grids(hfb.params.init_params(), nx=n, ny=n, nz=n, dx=d, dy=d, dz=d, periodic=periodic)
     x = (torch.arange(n, dtype=torch.float64, device="cuda") - (n - 1) / 2) * d
     r2 = x[:, None, None] ** 2 + x[None, :, None] ** 2 + (1.2 * x[None, None, :]) ** 2
     for call_no in range(2):           # two calls in a row share the one buffer
@@ -44,3 +47,5 @@ def test_poisson_noalloc_rejects_large_grid():
     w = torch.zeros((48, 48, 48), dtype=torch.float64, device="cuda")
     r = load().hfb_poisson_noalloc(g.ctx.handle, ptr(rho[1]), ptr(w), stream_ptr())
     assert r == 2   # HFB_ERR_UNSUPPORTED_GRID: the doubled 96^3 grid exceeds the fixed 64^3 buffer
+    torch.cuda.synchronize()
+    assert int(torch.count_nonzero(w)) == 0   # rejected before anything ran
