@@ -135,6 +135,28 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def workload_description(name):
+    """The workload's physics and sizes, from its preset."""
+    from hfb import config
+    c = config.case_dict(name)
+    g, f, lv = c["grid"], c["force"], c["levels"]
+    pairing = "no pairing" if f.get("ipair", 0) == 0 else "volume-delta pairing, 60 MeV soft window"
+    n = g["nx"]
+    coul = n if g.get("periodic") else 2 * n
+    return (f"{name} HF-BCS (N={lv['nneut']}, Z={lv['nprot']}): SLy4 + {pairing}, {n}^3 grid dx {g['dx']} fm, "
+            f"{lv['npsi'][0]}+{lv['npsi'][1]} 2-spinor states, HO start (beta {c.get('beta', 0.0)}), "
+            f"{coul}^3 Coulomb grid")
+
+
+def l2_note(st):
+    """Whether the timed iterations stream more than L2 (126 MB) per step."""
+    lv = st["levels"]
+    mb = lv.psi.numel() * 8 / 1e6   # complex64 states of the single-precision bulk
+    if mb > 126:
+        return f"inputs larger than L2: single-precision states {mb:.0f} MB (FP64 {2 * mb:.0f} MB), no flush"
+    return f"states {mb:.0f} MB (FP64 {2 * mb:.0f} MB) fit in L2: each iteration rewrites them several times; no flush"
+
+
 def _state(case_name, dtype):
     from hfb import config
     return config.setup(config.case_dict(case_name), dtype=dtype)
@@ -312,12 +334,58 @@ def oracle_iterations(case_name, n_iter, warm=1, budget_s=None, threads=None):
     return times, threads, desc
 
 
+def oracle_converged_run(case_name, tol_kev, max_iter, threads=None):
+    """The NumPy oracle from the oscillator start to convergence on the host
+    cores (the estimated remaining energy change below STOP_MEV, as the FP64
+    GPU leg): a measured CPU time-to-converge, for workloads small enough to
+    afford it.  Returns (seconds to |E - E_ref| <= tol, iterations to it,
+    iterations run, E_ref, threads)."""
+    sys.path.insert(0, ROOT)
+    from hfb import config, static as hst
+    from oracle import static as ost, pool
+    threads = threads or os.cpu_count() or 1
+    pool.set_workers(threads)
+    t0 = time.perf_counter()
+    rs = ost.build(config.case_dict(case_name))
+    ost.prepare(rs)
+    E, T = [], []
+    converged = False
+    for i in range(1, max_iter + 1):
+        ost.iterate(rs, i)
+        E.append(float(rs.en.ehf))
+        T.append(time.perf_counter() - t0)
+        rem = hst.remaining_change(E)
+        if i > 60 and rem is not None and abs(rem) < STOP_MEV:
+            converged = True
+            break
+    pool.set_workers(1)
+    if not converged:
+        return None, None, len(E), None, threads
+    e_ref = E[-1] + hst.remaining_change(E)
+    idx = converged_index(E, e_ref, tol_kev * 1e-3, [True] * len(E))
+    return T[idx], idx + 1, len(E), e_ref, threads
+
+
 def reference_arm(args, rank, world):
     """The reference's CPU path on the host cores.  JAX is not installable
     here, so this is the oracle port: whole iterations, timed one per step,
     scaled to the FP64 iteration count recorded for the workload."""
     if rank != 0:
         return None
+    if args.cpu_full:
+        t, it, nrun, e_ref, threads = oracle_converged_run(args.workload, args.tol_kev, args.max_iter)
+        return dict(metric=METRIC, value=t, unit=UNIT, n_gpus=args.gpus, steps=nrun, warmup=0,
+                    ms_per_step=(t / it * 1e3) if t else None, higher_is_better=False, scaling="weak",
+                    vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
+                    config=dict(workload=workload_description(args.workload) + ", FP64 NumPy oracle on host cores",
+                                step="one whole self-consistent iteration of the oracle",
+                                fp64_iterations_to_1kev=it, iterations_run=nrun, e_ref_mev=e_ref,
+                                measured="full run from the oscillator start to convergence (not extrapolated)"),
+                    cpu_baseline=dict(value=t, unit=UNIT, cores=threads, kind="port",
+                                      sample=f"full {args.workload} run of the NumPy FP64 oracle, {nrun} iterations, "
+                                             f"per-state work on {threads} host threads; restatement of the reference, "
+                                             "not its JAX code"),
+                    e2e=dict(value=t, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     times, threads, desc = oracle_iterations(args.workload, max(args.steps, 1), warm=min(max(args.warmup, 1), 2),
                                              budget_s=REFERENCE_ARM_BUDGET_S)
     per_it = statistics.median(times)
@@ -326,7 +394,7 @@ def reference_arm(args, rank, world):
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=len(times),
                 warmup=min(max(args.warmup, 1), 2), ms_per_step=per_it * 1e3, higher_is_better=False,
                 scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
-                config=dict(workload=f"{args.workload} HF-BCS (the bench workload), FP64 NumPy oracle on host cores",
+                config=dict(workload=workload_description(args.workload) + ", FP64 NumPy oracle on host cores",
                             step="one whole self-consistent iteration of the oracle",
                             fp64_iterations_to_1kev=iters,
                             iterations_source="FP64 GPU run of the same algorithm (bench FP64 leg)",
@@ -349,6 +417,9 @@ def main():
     ap.add_argument("--tol-kev", type=float, default=1.0)
     ap.add_argument("--max-iter", type=int, default=4000, help="iteration cap of each self-consistent run")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-full", action="store_true",
+                    help="reference arm: run the oracle to convergence (a measured CPU time-to-converge; small "
+                         "workloads only)")
     ap.add_argument("--switch-mev", type=float, default=5e-4,
                     help="mixed run: estimated remaining change (MeV) at which FP32 hands over to FP64")
     args = ap.parse_args()
@@ -425,11 +496,10 @@ def main():
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=steps, warmup=W,
         ms_per_step=(value / steps * 1e3) if value else None, higher_is_better=False,
         scaling="weak", vs_baseline=None, dtype="f32+f64", data="synthetic",
-        config=dict(workload=f"{args.workload} HF-BCS: SLy4 + volume-delta pairing, 48^3 grid dx 0.8 fm, "
-                             "140+96 2-spinor states, HO start, 96^3 Coulomb grid",
+        config=dict(workload=workload_description(args.workload),
                     step="one self-consistent iteration; steps = mixed iterations to |E - E_ref| <= tol",
                     parallelism="replicas" if world > 1 else "single GPU",
-                    l2="inputs larger than L2 (states 0.5-0.8 GB)", tolerance_kev=args.tol_kev,
+                    l2=l2_note(rm["state"]), tolerance_kev=args.tol_kev,
                     fp64_converged=r64["converged"], fp64_time_to_converge_s=t64,
                     fp64_iterations=(i64 + 1) if i64 is not None else None,
                     fp64_iterations_run=r64["iters"],

@@ -41,7 +41,8 @@ enum hfb_status {
                                    [-100, 100] (pairs.py:59 raises)      */
   HFB_ERR_NO_CONVERGENCE = 5,   /* Jacobi or Brent iteration limit       */
   HFB_ERR_NONFINITE = 6,        /* NaN / Inf in an energy or a norm      */
-  HFB_ERR_ALLOC = 7             /* device allocation failed              */
+  HFB_ERR_ALLOC = 7,            /* device allocation failed              */
+  HFB_ERR_TIMEOUT = 8           /* a bounded device wait ran out         */
 };
 
 enum hfb_precision { HFB_F64 = 0, HFB_F32 = 1 };
@@ -75,6 +76,19 @@ unsigned long long hfb_launch_count(void);
 const char* hfb_last_cuda_error(int* code);
 /* Latched device-side status (synchronises the stream), then clears it. */
 int hfb_device_status(hfb_ctx_t ctx, void* stream, int* status_out);
+
+/* Bound, in SM clock cycles, of any one wait inside the tensor-core kernels
+ * (an MMA completion, a copy, another CTA's tile); default 2e9 (about one
+ * second).  A wait that runs out latches HFB_ERR_TIMEOUT, the kernel waits
+ * for its own MMAs, releases its tensor memory and returns, and the context
+ * stays usable.  No counterpart in the reference (JAX has no device waits). */
+int hfb_set_wait_limit(hfb_ctx_t ctx, long long cycles);
+/* For tests of that path: the next single-precision tensor-core hpsi launch
+ * on this context has its first CTA wait, before it takes any work, on a
+ * device word nothing writes, so the wait runs out after the wait limit and
+ * the launch ends with HFB_ERR_TIMEOUT latched (no counterpart in the
+ * reference). */
+int hfb_arm_timeout_probe(hfb_ctx_t ctx);
 
 /* ---- levels.py --------------------------------------------------------- */
 /* cderv{x,y,z}00 / 01 / 02 (levels.py:132-395) on nsp spinors.
@@ -223,6 +237,59 @@ int hfb_eigh(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w, 
  * eigh of static.py:300-310 / 397-407. */
 int hfb_eigh_near_diagonal(hfb_ctx_t ctx, int nb, int n, int lda, const double* a, double* w,
                            double* v, void* stream);
+
+/* lastdiag (static.py:1072-1168): quasiparticle spectrum of one isospin
+ * block after convergence.  hmatrix and gapmatrix are complex [nst][ldh]
+ * (the block's corner of static.hmatrix / gapmatrix), wocc the nst BCS
+ * occupations of the block's states, eferm one device double (that
+ * isospin's Fermi energy), first the index of the block's first state in
+ * the whole state array (its parity picks the time-reversal partner in the
+ * lower-component coefficients).  Outputs: qp_energy[nst] ascending and
+ * qp_norm[nst], the norm of each eigenvector's lower component.  The
+ * reference passes nst = nneut / nprot and first = 0 / nneut; the Python
+ * mirror passes the isospin's whole block (npsi, npmin) unless asked for the
+ * reference's ranges. */
+int hfb_lastdiag(hfb_ctx_t ctx, int nst, int ldh, const double* hmatrix, const double* gapmatrix,
+                 const double* wocc, const double* eferm, int first, double* qp_energy, double* qp_norm,
+                 void* stream);
+
+/* hfb_natural (static.py:920-1070): configuration-space sub-iterations for
+ * one isospin block of nst states starting at state index ``start``.
+ * Matrices are the complex [2][ld][ld] static.hmatrix, gapmatrix, symcond,
+ * lambda_save (block iq); per-state arrays are over all states.  The host
+ * runs the reference's loop:
+ *   hfb_natural_begin                    cm = I, damping, h and gap at entry
+ *   for each sub-iteration:
+ *     hfb_natural_step(last)             gradient step on cm, QR (LAPACK
+ *                                        conventions), transformed h and gap,
+ *                                        sp_energy (and deltaf with pairing)
+ *     [BCS solve when pairing is on]
+ *     hfb_natural_symcond                (not after the last) new symcond
+ *   hfb_natural_end                      psi_out[block] = psi[block] cm,
+ *                                        lagrange[block] = psi cm htran, the
+ *                                        matrices of the block replaced
+ * The work matrices live in the context between these calls: one sequence
+ * at a time per context.  nst <= 256. */
+typedef struct hfb_natural_args {
+  int nst, ld, iq, start;  /* block size, matrix leading dim, isospin, first state */
+  int ipair, pad_;
+  double delstepbas, e0bas;
+  double* hmatrix;         /* complex [2][ld][ld] */
+  double* gapmatrix;
+  double* symcond;
+  double* lambda_save;
+  double* sp_energy;       /* [nstmax] */
+  double* deltaf;          /* [nstmax], may be NULL without pairing */
+  const double* wocc;
+  const double* wguv;
+  const double* pairwg;
+  const double* wstates;
+} hfb_natural_args;
+int hfb_natural_begin(hfb_ctx_t ctx, const hfb_natural_args* a, void* stream);
+int hfb_natural_step(hfb_ctx_t ctx, const hfb_natural_args* a, int last, void* stream);
+int hfb_natural_symcond(hfb_ctx_t ctx, const hfb_natural_args* a, void* stream);
+int hfb_natural_end(hfb_ctx_t ctx, int prec, const hfb_natural_args* a, const void* psi, void* psi_out,
+                    void* lagrange, void* stream);
 
 /* ---- pairs.py ---------------------------------------------------------- */
 typedef struct hfb_pair_args {

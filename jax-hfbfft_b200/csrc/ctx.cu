@@ -15,7 +15,8 @@ static thread_local int t_last_cuda_error = 0;
 void note_cuda_error(int e) { t_last_cuda_error = e; }
 
 int coulomb_init(hfb_ctx_s* c);  // skyrme.cu
-int hpsi_tc_prepare(hfb_ctx_s* c);  // hpsi_tc.cu
+int hpsi_tc_prepare(hfb_ctx_s* c);   // hpsi_tc.cu
+int hpsi_bf3_prepare(hfb_ctx_s* c);  // hpsi_bf3.cu
 
 void* scratch(hfb_ctx_s* c, int s, size_t bytes) {
   if (s < 0 || s >= hfb_ctx_s::S_NSLOT) return nullptr;
@@ -94,6 +95,14 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     c->use_tcgen05 = (e && e[0] == '1') ? 0 : 1;
     const char* j = getenv("HFB_LAMBDA_JACOBI");
     c->lambda_refine = (j && j[0] == '1') ? 0 : 1;
+    // single-precision hpsi kernel: HFB_HPSI_KERNEL=bf16x3 or tf32x3
+    const char* h = getenv("HFB_HPSI_KERNEL");
+    c->hpsi_kind = (h && strcmp(h, "bf16x3") == 0) ? 0 : 1;
+    // FP64 Gram contractions: HFB_GRAM_F64=dmma (FP64 tensor cores) or simt
+    const char* gk = getenv("HFB_GRAM_F64");
+    c->gram_f64_dmma = (gk && strcmp(gk, "dmma") == 0) ? 1 : 0;
+    c->wait_limit = kDefaultWaitLimit;
+    c->timeout_probe = 0;
   }
   const size_t nn = (size_t)nx * nx;
   for (int a = 0; a < 3; ++a) {
@@ -125,6 +134,7 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
   }
   int r = coulomb_init(c);
   if (r == HFB_OK) r = hpsi_tc_prepare(c);
+  if (r == HFB_OK) r = hpsi_bf3_prepare(c);
   if (r == HFB_OK && cudaDeviceSynchronize() != cudaSuccess) r = HFB_ERR_CUDA;
   if (r != HFB_OK) {
     hfb_ctx_destroy(c);
@@ -143,6 +153,7 @@ extern "C" int hfb_ctx_destroy(hfb_ctx_t c) {
   }
   if (c->coul_q) cudaFree(c->coul_q);
   if (c->hpsi_b) cudaFree(c->hpsi_b);
+  if (c->hpsi_bf3_b) cudaFree(c->hpsi_bf3_b);
   if (c->dev_status) cudaFree(c->dev_status);
   if (c->side) {
     cudaStreamDestroy(c->side);
@@ -173,8 +184,21 @@ extern "C" const char* hfb_status_string(int s) {
     case HFB_ERR_NO_CONVERGENCE: return "iteration limit reached (Jacobi / Newton-Schulz / Brent)";
     case HFB_ERR_NONFINITE: return "non-finite value";
     case HFB_ERR_ALLOC: return "device allocation failed";
+    case HFB_ERR_TIMEOUT: return "a bounded device wait ran out (tensor-core pipeline)";
     default: return "unknown status";
   }
+}
+
+extern "C" int hfb_set_wait_limit(hfb_ctx_t c, long long cycles) {
+  if (!c || cycles <= 0) return HFB_ERR_ARG;
+  c->wait_limit = cycles;
+  return HFB_OK;
+}
+
+extern "C" int hfb_arm_timeout_probe(hfb_ctx_t c) {
+  if (!c) return HFB_ERR_ARG;
+  c->timeout_probe = 1;
+  return HFB_OK;
 }
 
 extern "C" int hfb_device_status(hfb_ctx_t c, void* stream, int* status_out) {

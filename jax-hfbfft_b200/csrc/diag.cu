@@ -112,6 +112,130 @@ gram_kernel(GramJob job, size_t K, size_t n3, const cplx<R>* __restrict__ psi, c
       o[(ty + 12 * u) * GT + tx + 16 * v] = make_double2((double)acc[u][v][0], (double)acc[u][v][1]);
 }
 
+// FP64 states: the same tiles, split-K chunks and partial layout on the
+// FP64 tensor cores (mma.sync m8n8k4 .f64).  Over the interleaved storage,
+// with k' running over (Re, Im) of each element,
+//   Re C_ij = sum_k' a_ik' b_jk',   a = psi_i, b = x_j,
+//   Im C_ij = sum_k' a_ik' bt_jk',  bt = (Im x, -Re x) per element,
+// so each 8 x 8 output block takes two real MMAs per four k'; bt is b with
+// the partner lane's value (one shuffle).  A CTA (4 warps, 24 x 24 outputs
+// per warp, 3 x 3 MMA blocks) streams K in stages of GD_KB elements through
+// cp.async double buffers (rows padded by one element: the 8 rows a
+// fragment load touches fall on distinct bank groups).
+constexpr int GD_KB = 16;              // complex k per shared-memory stage
+constexpr int GD_LD = GD_KB + 1;       // padded row length (complex)
+constexpr int GD_THREADS = 128;
+constexpr size_t GD_SMEM = sizeof(double2) * 2 * 2 * GT * GD_LD;
+
+__device__ __forceinline__ void gd_cp16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+
+__device__ __forceinline__ void gd_mma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(GD_THREADS) gram_dmma_kernel(GramJob job, size_t K, size_t n3,
+                                                                const double2* __restrict__ psi,
+                                                                const double2* __restrict__ hampsi,
+                                                                const double2* __restrict__ hmfpsi, double2* part,
+                                                                int nchunk) {
+  extern __shared__ double2 gd_smem[];
+  double2* As = gd_smem;                 // [2][GT][GD_LD]
+  double2* Bs = gd_smem + 2 * GT * GD_LD;
+  const GramTile tl = job.t[blockIdx.x];
+  const int b = tl.b, am = tl.a;
+  const int ns = job.ns[b];
+  const int i0 = tl.ti * GT, j0 = tl.tj * GT;
+  const double2* P = psi + (size_t)job.s0[b] * K;
+  const double2* X = am == 1 ? hampsi + (size_t)job.s0[b] * K : am == 2 ? hmfpsi + (size_t)job.s0[b] * K : P;
+  const double* vp = job.vp[b];
+  const size_t k0 = (size_t)blockIdx.y * GCHUNK;
+  const size_t k1 = min(K, k0 + GCHUNK);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rw = warp >> 1, cw = warp & 1;
+  const int fr = lane >> 2, fk = lane & 3;   // fragment row (A) / column (B), k' within the 4
+  double accR[3][3][2], accI[3][3][2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) accR[i][j][0] = accR[i][j][1] = accI[i][j][0] = accI[i][j][1] = 0.0;
+  // one stage: GT rows x GD_KB elements of each operand, consecutive
+  // threads on consecutive elements of a row (coalesced)
+  auto load = [&](int buf, size_t kb) {
+#pragma unroll
+    for (int h = 0; h < GT * GD_KB / GD_THREADS; ++h) {
+      const int e = threadIdx.x + GD_THREADS * h;
+      const int r = e / GD_KB, kk = e % GD_KB;
+      const size_t k = kb + kk;
+      double2* da = As + ((size_t)buf * GT + r) * GD_LD + kk;
+      double2* db = Bs + ((size_t)buf * GT + r) * GD_LD + kk;
+      const int gi = i0 + r, gj = j0 + r;
+      if (k < k1 && gi < ns) gd_cp16(da, P + (size_t)gi * K + k);
+      else *da = make_double2(0.0, 0.0);
+      if (k < k1 && gj < ns) {
+        if (am == 3) {
+          const double2 v = X[(size_t)gj * K + k];
+          const double w = vp[k % n3];
+          *db = make_double2(w * v.x, w * v.y);
+        } else {
+          gd_cp16(db, X + (size_t)gj * K + k);
+        }
+      } else {
+        *db = make_double2(0.0, 0.0);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  load(0, k0);
+  int buf = 0;
+  for (size_t kb = k0; kb < k1; kb += GD_KB) {
+    if (kb + GD_KB < k1) {
+      load(buf ^ 1, kb + GD_KB);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();
+    const double* A = reinterpret_cast<const double*>(As + (size_t)buf * GT * GD_LD);
+    const double* B = reinterpret_cast<const double*>(Bs + (size_t)buf * GT * GD_LD);
+#pragma unroll 4
+    for (int ks = 0; ks < GD_KB / 2; ++ks) {
+      const int kd = 2 * (2 * ks) + fk;      // double index of k' in the row
+      double a[3], bv[3], bt[3];
+#pragma unroll
+      for (int mi = 0; mi < 3; ++mi) a[mi] = A[(24 * rw + 8 * mi + fr) * (2 * GD_LD) + kd];
+#pragma unroll
+      for (int nj = 0; nj < 3; ++nj) {
+        bv[nj] = B[(24 * cw + 8 * nj + fr) * (2 * GD_LD) + kd];
+        const double o = __shfl_xor_sync(0xffffffffu, bv[nj], 1);
+        bt[nj] = (fk & 1) ? -o : o;
+      }
+#pragma unroll
+      for (int mi = 0; mi < 3; ++mi)
+#pragma unroll
+        for (int nj = 0; nj < 3; ++nj) {
+          gd_mma(accR[mi][nj], a[mi], bv[nj]);
+          gd_mma(accI[mi][nj], a[mi], bt[nj]);
+        }
+    }
+    __syncthreads();
+    buf ^= 1;
+  }
+  double2* o = part + ((size_t)blockIdx.x * nchunk + blockIdx.y) * GT * GT;
+#pragma unroll
+  for (int mi = 0; mi < 3; ++mi)
+#pragma unroll
+    for (int nj = 0; nj < 3; ++nj)
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+        o[(24 * rw + 8 * mi + fr) * GT + 24 * cw + 8 * nj + 2 * fk + i] = make_double2(accR[mi][nj][i], accI[mi][nj][i]);
+}
+
 struct GramOut {
   double2* p[8];   // [block * 4 + matrix]
 };
@@ -183,7 +307,14 @@ int gram_launch(hfb_ctx_s* c, int prec, int nblk, const int* s0, const int* ns, 
   GramOut ot;
   for (int q = 0; q < 8; ++q) ot.p[q] = outs_host[q];
   dim3 grid(job.ntile, nchunk);
-  if (prec == HFB_F64)
+  if (prec == HFB_F64 && c->gram_f64_dmma) {
+    static const bool smem_ok =
+        cudaFuncSetAttribute(gram_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GD_SMEM) ==
+        cudaSuccess;
+    if (!smem_ok) return HFB_ERR_CUDA;
+    gram_dmma_kernel<<<grid, GD_THREADS, GD_SMEM, st>>>(job, K, n3, (const double2*)psi, (const double2*)hampsi,
+                                                     (const double2*)hmfpsi, part, nchunk);
+  } else if (prec == HFB_F64)
     gram_kernel<double><<<grid, GTHREADS, 0, st>>>(job, K, n3, (const double2*)psi, (const double2*)hampsi,
                                               (const double2*)hmfpsi, part, nchunk);
   else
@@ -632,6 +763,15 @@ static int zgemm_small(int nmax, int ld, int ta, int tb, const double2* A, size_
                                                     gate_k);
   HFB_CHECK_LAUNCH();
   return HFB_OK;
+}
+
+// One n x n product C = A' B' (A' = A or A^H, B' = B or B^H), leading
+// dimension ld, for other translation units.
+int zgemm_small_one(int n, int ld, int ta, int tb, const double2* A, const double2* B, double2* C, cudaStream_t st) {
+  Pair2 nper;
+  nper.v[0] = n;
+  nper.v[1] = 0;
+  return zgemm_small(n, ld, ta, tb, A, 0, B, 0, C, 0, nper, 1, st);
 }
 
 // ------------------------------------------ Hermitian eigen refinement ----

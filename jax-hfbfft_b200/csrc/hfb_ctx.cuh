@@ -22,14 +22,24 @@ struct hfb_ctx_s {
   int lambda_refine;     // FP64 diagstep diagonalises lambda by eigen refinement (default 1;
                          // HFB_LAMBDA_JACOBI=1 at creation selects the Jacobi solver)
   cudaEvent_t ev_fork, ev_join;
-  unsigned char* hpsi_b; // single-precision hpsi: derivative matrices in the tensor-core tile layout
+  unsigned char* hpsi_b; // single-precision hpsi (tf32 kernel): derivative matrices in the tensor-core tile layout
+  unsigned char* hpsi_bf3_b; // single-precision hpsi (bf16 three-term kernel): the same, bf16 h/m/l tiles
+  int hpsi_kind;         // single-precision hpsi kernel: 0 bf16 three-term, 1 tf32 three-term
+                         // (HFB_HPSI_KERNEL=bf16x3 / tf32x3 in the environment at creation)
+  int gram_f64_dmma;     // FP64 Gram on the FP64 tensor cores (HFB_GRAM_F64=dmma) or CUDA cores
+  long long wait_limit;  // clock cycles any one bounded device wait may take (hfb_set_wait_limit)
+  int timeout_probe;     // the next tensor-core hpsi launch runs its timeout path (hfb_arm_timeout_probe)
   // scratch arena: fixed slots, grown on demand (never shrunk)
-  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_HPT, S_NSLOT };
+  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_HPT, S_LAST, S_NAT, S_NSLOT };
   void* slot[S_NSLOT];
   size_t slot_bytes[S_NSLOT];
 };
 
 namespace hfb {
+
+// Default bound of any one device-side wait of the tensor-core pipelines
+// (about one second at the B200's clocks); hfb_set_wait_limit changes it.
+constexpr long long kDefaultWaitLimit = 2000000000LL;
 
 // Scratch buffer ``s`` of at least ``bytes``; nullptr on allocation failure.
 void* scratch(hfb_ctx_s* c, int s, size_t bytes);

@@ -326,11 +326,16 @@ int hpsi_launch_t(hfb_ctx_s* c, const void* pot, int s0, int ns, int nneut, cons
   return HFB_OK;
 }
 
-int hpsi_ovl_parts(hfb_ctx_s* c, int prec) { return hpsi_tc_available(c, prec) ? hpsi_tc_parts(c) : c->n; }
+int hpsi_ovl_parts(hfb_ctx_s* c, int prec) {
+  if (hpsi_bf3_available(c, prec)) return hpsi_bf3_parts(c);
+  return hpsi_tc_available(c, prec) ? hpsi_tc_parts(c) : c->n;
+}
 
 int hpsi_launch(hfb_ctx_s* c, int prec, const void* pot, int s0, int ns, int nneut, const void* psi,
                 const double* weight, const double* weightuv, void* acc, void* pout, void* pout_mf, void* pout_del,
                 double* ovl, cudaStream_t st) {
+  if (hpsi_bf3_available(c, prec))
+    return hpsi_bf3_launch(c, pot, s0, ns, nneut, psi, weight, weightuv, acc, pout, pout_mf, pout_del, ovl, st);
   if (hpsi_tc_available(c, prec))
     return hpsi_tc_launch(c, pot, s0, ns, nneut, psi, weight, weightuv, acc, pout, pout_mf, pout_del, ovl, st);
   return dispatch_n(c->n, [&](auto nn) -> int {

@@ -21,6 +21,14 @@ int hpsi_tc_launch(hfb_ctx_s* c, const void* pot, int s0, int ns, int nneut, con
                    const double* weightuv, void* acc, void* pout, void* pout_mf, void* pout_del, double* ovl,
                    cudaStream_t st);
 
+// The same on the bf16 three-term kernel (hpsi_bf3.cu), two CTAs per SM.
+int hpsi_bf3_prepare(hfb_ctx_s* c);
+bool hpsi_bf3_available(hfb_ctx_s* c, int prec);
+int hpsi_bf3_parts(hfb_ctx_s* c);
+int hpsi_bf3_launch(hfb_ctx_s* c, const void* pot, int s0, int ns, int nneut, const void* psi, const double* weight,
+                    const double* weightuv, void* acc, void* pout, void* pout_mf, void* pout_del, double* ovl,
+                    cudaStream_t st);
+
 // Partial sums per state that hpsi_launch writes into ``ovl``.
 int hpsi_ovl_parts(hfb_ctx_s* c, int prec);
 

@@ -13,11 +13,13 @@ LIB_PATH = os.path.join(_HERE, "libhfb.so")
 
 HFB_OK = 0
 HFB_ERR_CUDA = 3
+HFB_ERR_NONFINITE = 6
+HFB_ERR_TIMEOUT = 8
 HFB_F64 = 0
 HFB_F32 = 1
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported grid", 3: "CUDA error",
           4: "BCS particle number not bracketed on [-100, 100]", 5: "iteration limit reached",
-          6: "non-finite value", 7: "device allocation failed"}
+          6: "non-finite value", 7: "device allocation failed", 8: "a bounded device wait ran out"}
 ENERGY_KEYS = ("ehft", "ehf0", "ehf1", "ehf2", "ehf3", "ehfls", "ehflsodd", "ehfc", "ecorc", "ehfint",
                "e3corr", "e_zpe", "ehf", "tke", "ehfCrho0", "ehfCrho1", "ehfCdrho0", "ehfCdrho1",
                "ehfCtau0", "ehfCtau1", "ehfCdJ0", "ehfCdJ1", "ehfCj0", "ehfCj1")
@@ -63,12 +65,21 @@ class PairArgs(C.Structure):
                 ("out", vp)]
 
 
+class NaturalArgs(C.Structure):
+    _fields_ = [("nst", C.c_int), ("ld", C.c_int), ("iq", C.c_int), ("start", C.c_int), ("ipair", C.c_int),
+                ("pad_", C.c_int), ("delstepbas", C.c_double), ("e0bas", C.c_double),
+                ("hmatrix", vp), ("gapmatrix", vp), ("symcond", vp), ("lambda_save", vp), ("sp_energy", vp),
+                ("deltaf", vp), ("wocc", vp), ("wguv", vp), ("pairwg", vp), ("wstates", vp)]
+
+
 # symbol -> argument types (restype int unless noted)
 _PROTOS = {
     "hfb_ctx_create": [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                        C.POINTER(vp)],
     "hfb_ctx_destroy": [vp],
     "hfb_device_status": [vp, vp, C.POINTER(C.c_int)],
+    "hfb_set_wait_limit": [vp, C.c_longlong],
+    "hfb_arm_timeout_probe": [vp],
     "hfb_cderv": [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
     "hfb_laplace": [vp, C.c_int, C.c_int, vp, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp],
     "hfb_hpsi": [vp, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp],
@@ -85,6 +96,11 @@ _PROTOS = {
     "hfb_eigh": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
     "hfb_eigh_near_diagonal": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp],
     "hfb_pair": [vp, C.POINTER(PairArgs), vp],
+    "hfb_lastdiag": [vp, C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, vp],
+    "hfb_natural_begin": [vp, C.POINTER(NaturalArgs), vp],
+    "hfb_natural_step": [vp, C.POINTER(NaturalArgs), C.c_int, vp],
+    "hfb_natural_symcond": [vp, C.POINTER(NaturalArgs), vp],
+    "hfb_natural_end": [vp, C.c_int, C.POINTER(NaturalArgs), vp, vp, vp, vp],
     "hfb_energies": [vp, C.POINTER(HfbForce), C.c_int, C.c_double] + [vp] * 6 + [vp, vp, vp],
     "hfb_sum_energy": [vp, C.c_int] + [vp] * 6 + [vp, vp],
     "hfb_energy_grad": [vp, C.POINTER(HfbForce)] + [vp] * 5 + [vp, vp],

@@ -13,7 +13,7 @@ import time
 import torch
 
 from . import _lib
-from ._lib import call, ptr, stream_ptr, prec_of, GrstepArgs, DiagArgs
+from ._lib import call, ptr, stream_ptr, prec_of, GrstepArgs, DiagArgs, NaturalArgs
 from .densities import add_density
 from .meanfield import skyrme
 from .pairs import pair
@@ -166,6 +166,76 @@ def diagstep(energies, forces, grids, levels, static, diagonalize=False, constru
     return energies, levels, static
 
 
+def lastdiag(forces, grids, levels, params, static, pairs, isospin, reference_indexing=False):
+    """Quasiparticle energies (ascending) and lower-component norms of one
+    isospin after convergence (static.py:1072-1168), from the h and gap
+    matrices of the last diagonalisation step, the occupations and the
+    Fermi energy; returns two device tensors.  By default the isospin's
+    whole block of states is used (start npmin, npsi states).  The
+    reference takes the first nneut / nprot states from index 0 / nneut
+    (static.py:1074-1084), which for protons is not the proton block unless
+    nneut == npsi[0]; ``reference_indexing=True`` restates those ranges."""
+    lv = levels
+    if reference_indexing:
+        nst = lv.nneut if isospin == 0 else lv.nprot
+        start = 0 if isospin == 0 else lv.nneut
+    else:
+        nst = lv.npsi[isospin]
+        start = 0 if isospin == 0 else lv.npsi[0]
+    ld = static.hmatrix.shape[-1]
+    if nst > ld or start + nst > lv.nstmax:
+        raise ValueError(f"lastdiag: {nst} states from {start} do not fit the matrices ({ld}) / states")
+    e = torch.empty(nst, dtype=torch.float64, device="cuda")
+    q = torch.empty(nst, dtype=torch.float64, device="cuda")
+    w = lv.wocc[start:start + nst].contiguous()
+    call("hfb_lastdiag", grids.ctx.handle, nst, ld, ptr(static.hmatrix[isospin]), ptr(static.gapmatrix[isospin]),
+         ptr(w), ptr(pairs.out[0, isospin:isospin + 1].contiguous()), start, ptr(e), ptr(q), stream_ptr())
+    return e, q
+
+
+def hfb_natural(forces, grids, levels, meanfield, params, static, isospin, iternat, pairs=None,
+                reference_indexing=False):
+    """Configuration-space sub-iterations (static.py:920-1070): a damped
+    gradient step on a unitary transformation of the isospin's states driven
+    by symcond, orthonormalised by QR, the h and gap matrices transformed;
+    at the end the states and Lagrange fields are rotated and the block's
+    matrices replaced.  With pairing the BCS solver runs between
+    sub-iterations -- here ``pair()`` with ``pairs`` (the reference's
+    single-isospin call, static.py:988, lacks an argument and its last call
+    passes no pairs object; the other isospin's inputs are unchanged, so
+    solving both is the same as solving one).  Block: the isospin's whole
+    block (npmin, npsi) by default, the reference's ranges (first nneut /
+    nprot states from 0 / nneut) with ``reference_indexing=True``.  Like the
+    reference, the Lagrange fields become psi_new htran (static.py:1018)."""
+    lv = levels
+    if reference_indexing:
+        nst = lv.nneut if isospin == 0 else lv.nprot
+        start = 0 if isospin == 0 else lv.nneut
+    else:
+        nst = lv.npsi[isospin]
+        start = 0 if isospin == 0 else lv.npsi[0]
+    a = NaturalArgs()
+    a.nst, a.ld, a.iq, a.start = nst, static.hmatrix.shape[-1], int(isospin), start
+    a.ipair = int(forces.ipair != 0)
+    a.delstepbas, a.e0bas = float(static.delstepbas), float(static.e0bas)
+    a.hmatrix, a.gapmatrix = ptr(static.hmatrix), ptr(static.gapmatrix)
+    a.symcond, a.lambda_save = ptr(static.symcond), ptr(static.lambda_save)
+    a.sp_energy, a.deltaf = ptr(lv.sp_energy), ptr(lv.deltaf)
+    a.wocc, a.wguv, a.pairwg, a.wstates = ptr(lv.wocc), ptr(lv.wguv), ptr(lv.pairwg), ptr(lv.wstates)
+    h = grids.ctx.handle
+    call("hfb_natural_begin", h, a, stream_ptr())
+    for it in range(iternat):
+        last = it == iternat - 1
+        call("hfb_natural_step", h, a, int(last), stream_ptr())
+        if forces.ipair != 0 and pairs is not None:
+            pair(levels, meanfield, forces, params, grids, pairs)
+        if not last:
+            call("hfb_natural_symcond", h, a, stream_ptr())
+    call("hfb_natural_end", h, prec_of(lv.psi), a, ptr(lv.psi), ptr(lv.psi_spare), ptr(lv.lagrange), stream_ptr())
+    lv.psi[start:start + nst].copy_(lv.psi_spare[start:start + nst])
+    return levels, static
+
+
 @dataclass
 class RunResult:
     history: list = field(default_factory=list)
@@ -232,7 +302,9 @@ def iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, p
     if forces.ipair != 0:
         pair(levels, meanfield, forces, params, grids, pairs)
     if forces.ipair != 0 and static.iternat > 0 and i > static.iternat_start and not forces.tbcs:
-        raise NotImplementedError("hfb_natural sub-iterations (static.py:920-1070) are not part of the hot path")
+        # configuration-space sub-iterations (static.py:1796-1798)
+        for iq in range(2):
+            hfb_natural(forces, grids, levels, meanfield, params, static, iq, static.iternat, pairs=pairs)
     # densities with mixing 0.2 new + 0.8 old for rho, tau, chi, and the
     # kinetic energies of sp_properties from the same derivatives
     add_density(densities, grids, levels, mix=0.2, forces=forces)

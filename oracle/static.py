@@ -304,6 +304,11 @@ def iterate(rs, i, x0_schedule=None):
     rs.en, lv, st = diagstep(rs.en, f, g, lv, st, st.tdiag, True)
     if f.ipair != 0:
         lv, rs.pairs = pair(lv, rs.mf, f, i, g, rs.pairs)
+    if f.ipair != 0 and st.iternat > 0 and i > st.iternat_start and not f.tbcs:   # (1796-1798)
+        def hook(levels):
+            _, rs.pairs = pair(levels, rs.mf, f, i, g, rs.pairs)
+        for iq in range(2):
+            lv, st = hfb_natural(lv, st, iq, st.iternat, ipair=f.ipair, pair_hook=hook)
     old = (rs.dens.rho.copy(), rs.dens.tau.copy(), rs.dens.chi.copy())
     rs.dens = add_density(rs.dens, g, lv)
     addnew = 0.2
@@ -365,3 +370,118 @@ def run(rs, maxiter=None, callback=None):
         if done:
             break
     return rs
+
+
+def lastdiag_block(h, gap, w, eferm, first):
+    """Quasiparticle energies and lower-component norms of one block
+    (static.py:1072-1168).  ``h``, ``gap``: the block's (nst, nst) corners of
+    the h and gap matrices; ``w``: the occupations of the block's states;
+    ``first``: the index of the block's first state in the whole state array
+    (the parity of a state's index picks its time-reversal partner,
+    static.py:1129-1139).  Returns (energies ascending, norms)."""
+    nst = h.shape[0]
+    wi, wj = w[:, None], w[None, :]
+    xi = -np.sqrt(wi * wj) + np.sqrt((1.0 - wi) * (1.0 - wj))                # (1105-1106)
+    eta = np.sqrt(wi * (1.0 - wj)) + np.sqrt(wj * (1.0 - wi))                 # (1108-1109)
+    hm = h - eferm * np.eye(nst)                                              # (1116-1117)
+    m = hm * xi + gap * eta                                                   # (1120)
+    e, u = np.linalg.eigh(m, UPLO="L")                                        # (1124)
+    c = np.zeros((nst, nst))
+    for i in range(nst):                                                      # (1129-1139)
+        g = first + i
+        if g % 2 == 0 and i >= 1:
+            c[i, i - 1] = -np.sqrt(w[i])
+        if g % 2 == 1 and i + 1 < nst:
+            c[i, i + 1] = np.sqrt(w[i])
+    low = c @ u
+    norm = np.sqrt(np.sum(np.abs(low) ** 2, axis=0))                          # (1142-1148)
+    order = np.argsort(e, kind="stable")                                      # (1151-1153)
+    return e[order], norm[order]
+
+
+def lastdiag(levels, st, eferm, iq, reference_indexing=False):
+    """lastdiag for isospin ``iq``.  The reference takes the first nneut
+    (nprot) states starting at index 0 (nneut), static.py:1074-1084: for
+    protons that is not the proton block unless nneut == npsi[0], and it
+    leaves out the unoccupied states of each block.  By default the whole
+    block of the isospin is used (start npmin, size npsi);
+    ``reference_indexing=True`` restates the reference's ranges."""
+    if reference_indexing:
+        nst = levels.nneut if iq == 0 else levels.nprot
+        start = 0 if iq == 0 else levels.nneut
+    else:
+        nst = levels.npsi[iq]
+        start = 0 if iq == 0 else levels.npsi[0]
+    return lastdiag_block(st.hmatrix[iq, :nst, :nst], st.gapmatrix[iq, :nst, :nst],
+                          np.asarray(levels.wocc)[start:start + nst], float(eferm[iq]), start)
+
+
+def calc_lambda(h, gap, wt, wu):
+    """Symmetric lambda of the sub-iterations (static.py:1030-1046):
+    lambda_temp[:, j] = wt_j h[:, j] - wu_j gap[:, j], lambda = (lt + lt^H)/2."""
+    lt = h * wt[None, :] - gap * wu[None, :]
+    return 0.5 * (lt + np.conj(lt.T))
+
+
+def hfb_natural(levels, st, iq, iternat, ipair=0, pair_hook=None, reference_indexing=False):
+    """Configuration-space sub-iterations (static.py:920-1070): a damped
+    gradient step on the unitary transformation ``cm`` driven by symcond,
+    orthonormalised by QR, the h and gap matrices transformed, and at the end
+    the states and Lagrange fields rotated.  With ``ipair != 0`` the
+    reference calls the pairing solver between sub-iterations
+    (``pair_hook(levels)``; its single-isospin call, static.py:988, has the
+    wrong number of arguments, and the last one passes no pairs object).
+    The block: the isospin's whole block by default; the reference's ranges
+    (first nneut / nprot states from index 0 / nneut) with
+    ``reference_indexing=True``.  The reference passes the transformed h
+    (not lambda) to the Lagrange-field update (static.py:1018, 1048-1068);
+    restated as written."""
+    if reference_indexing:
+        nst = levels.nneut if iq == 0 else levels.nprot
+        start = 0 if iq == 0 else levels.nneut
+    else:
+        nst = levels.npsi[iq]
+        start = 0 if iq == 0 else levels.npsi[0]
+    sl = slice(start, start + nst)
+    cm = np.eye(nst, dtype=np.complex128)
+    spe = levels.sp_energy
+    if st.e0bas == 0.0:
+        dampstep = np.full(nst, st.delstepbas / (np.max(spe[sl]) - np.min(spe[sl])))
+    else:
+        dampstep = st.delstepbas / (spe[sl] - spe[start] + st.e0bas)
+    hmat = st.hmatrix[iq, :nst, :nst].copy()
+    gapmat = st.gapmatrix[iq, :nst, :nst].copy()
+
+    def weights():
+        wt = levels.wocc[sl] * levels.wstates[sl]
+        wu = levels.wguv[sl] * levels.pairwg[sl] * levels.wstates[sl]
+        return wt, wu
+
+    htran = gaptran = None
+    for it in range(iternat):
+        cm = cm - dampstep[:, None] * st.symcond[iq, :nst, :nst]                  # (952-957)
+        cm, _ = np.linalg.qr(cm)                                                   # (959-960)
+        htran = np.conj(cm.T) @ hmat @ cm                                          # (964-965)
+        gaptran = np.conj(cm.T) @ gapmat @ cm
+        hcm = hmat @ cm                                                            # (968-969)
+        gapcm = gapmat @ cm
+        if ipair != 0 or it == iternat - 1:                                        # (972-992)
+            levels.sp_energy[sl] = np.diag(htran).real
+            if ipair != 0:
+                levels.deltaf[sl] = np.diag(gaptran).real * levels.pairwg[sl]
+                if pair_hook is not None:
+                    pair_hook(levels)
+        if it < iternat - 1:                                                       # (994-1015)
+            wt, wu = weights()
+            cml = cm @ calc_lambda(htran, gaptran, wt, wu)
+            st.symcond[iq, :nst, :nst] = hcm * wt[None, :] - gapcm * wu[None, :] - cml
+    shp = levels.psi[sl].shape
+    old = levels.psi[sl].reshape(nst, -1)                                          # (1018, 1048-1068)
+    new = cm.T @ old
+    levels.psi[sl] = new.reshape(shp)
+    levels.lagrange[sl] = (htran.T @ new).reshape(shp)
+    st.hmatrix[iq, :nst, :nst] = htran                                             # (1021-1022)
+    st.gapmatrix[iq, :nst, :nst] = gaptran
+    wt, wu = weights()
+    st.lambda_save[iq, :nst, :nst] = calc_lambda(htran, gaptran, wt, wu)           # (1025-1026)
+    return levels, st

@@ -31,3 +31,18 @@ RUN_CASES = {
                                      x0dmp=0.45, e0dmp=100.0, tvaryx_0=True, iternat=0),
                          mprint=1),
 }
+
+
+# The bench workloads (hfb.config presets, same inputs on both sides) run by
+# the reference driver for a bounded number of iterations: O16 (24^3, 10 + 10
+# states, no pairing) to the workload's iteration cap of 500, Cr48 (32^3,
+# 32 + 32 states, VDI, beta = 0.2) for its first 20 iterations, Pb208 (48^3,
+# 140 + 96 states, VDI) for its first 3.  The fixtures keep per-iteration
+# scalars, final single-particle quantities, radii and the inputs and
+# outputs of the reference's post-loop lastdiag -- no states, so they stay
+# small.
+CONFIG_RUNS = {
+    "o16_n24": dict(workload="O16", maxiter=500),
+    "cr48_n32": dict(workload="Cr48", maxiter=20),
+    "pb208_n48": dict(workload="Pb208", maxiter=3),
+}

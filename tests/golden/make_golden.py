@@ -19,7 +19,12 @@ the runs' final densities and on a seeded triaxial density; needs the run
 fixtures, ``--only observables`` regenerates it alone) and
 ``tests/golden/res_files.json`` (the text of the reference's .res writers
 for seeded inputs, ``--only res``) and ``tests/golden/constraint_n16.npz``
-(the reference's constraint module on seeded inputs, ``--only constraint``).
+(the reference's constraint module on seeded inputs, ``--only constraint``)
+and ``tests/golden/config_<case>.npz`` (the bench workloads through the
+reference driver for a bounded number of iterations, with its post-loop
+``lastdiag``; ``--only config`` or ``--only <case>``) and
+``tests/golden/natural_n8.npz`` (the reference's hfb_natural on seeded
+inputs, ``--only natural``).
 """
 import argparse
 import contextlib
@@ -33,7 +38,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
-from cases import RUN_CASES  # noqa: E402  (shared with the tests)
+from cases import RUN_CASES, CONFIG_RUNS  # noqa: E402  (shared with the tests)
 
 
 def _import_reference(ref):
@@ -112,6 +117,133 @@ def run_case(m, ref, name, case):
         ehf=float(en.ehf), ehfint=float(en.ehfint),
         upot=np.asarray(mf.upot), wcoul=np.asarray(coul.wcoul))
     print(f"{name}: {len(hist)} energy records, ehf={en.ehf:.10f}")
+
+
+def config_run(m, ref, name, workload, maxiter):
+    """A bench workload (hfb.config preset) through the reference driver
+    ``statichf_with_benchmark`` for ``maxiter`` iterations.  Records the
+    per-iteration scalars, the final single-particle energies, occupations
+    and radii, and the post-loop ``lastdiag`` of each isospin: its inputs
+    (h and gap matrices, occupations, Fermi energies) and its quasiparticle
+    energies and lower-component norms."""
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "jax-hfbfft_b200"))
+    from hfb import config   # the workload presets (plain Python data; nothing is computed by hfb here)
+    case = config.case_dict(workload, static=dict(maxiter=maxiter, iternat=0))
+    params, forces, grids, dens, mf, levels, static, coul, en, moment, pairs = _setup(m, ref, case)
+    levels = m["static"].harmosc(grids, levels, params, static)
+    hist = []
+    st_mod = m["static"]
+    orig_sum, orig_last = st_mod.sum_energy, st_mod.lastdiag
+    lastd = {}
+
+    def recording_sum_energy(energies, lv, meanfield, pr):
+        e = orig_sum(energies, lv, meanfield, pr)
+        hist.append((params.iteration, float(e.ehf), float(e.ehfint), float(e.efluct1[0]), float(e.efluct2[0]),
+                     float(static.x0dmp), float(np.sum(pr.epair))))
+        return e
+
+    def recording_lastdiag(f, g, lv, pa, stc, pr, iq):
+        if iq == 0:
+            lastd["hmatrix"] = np.array(stc.hmatrix)
+            lastd["gapmatrix"] = np.array(stc.gapmatrix)
+            lastd["wocc"] = np.array(lv.wocc)
+            lastd["eferm"] = np.array(pr.eferm)
+        qe, qn = orig_last(f, g, lv, pa, stc, pr, iq)
+        lastd[f"qp_energy_{iq}"], lastd[f"qp_norm_{iq}"] = np.asarray(qe), np.asarray(qn)
+        return qe, qn
+
+    st_mod.sum_energy = recording_sum_energy
+    st_mod.lastdiag = recording_lastdiag
+    tmp = tempfile.mkdtemp()
+    cwd = os.getcwd()
+    os.chdir(tmp)
+    try:
+        with contextlib.redirect_stdout(io.StringIO()):
+            out = st_mod.statichf_with_benchmark(coul, dens, en, forces, grids, levels, mf, moment, params,
+                                                 static, pairs, m["output"].FortranOutputWriter(tmp))
+    finally:
+        os.chdir(cwd)
+        st_mod.sum_energy, st_mod.lastdiag = orig_sum, orig_last
+    coul, dens, en, forces, grids, levels, mf = out[:7]
+    with contextlib.redirect_stdout(io.StringIO()):
+        obs = m["output"].calculate_complete_observables(dens, levels, grids, params)
+    h = np.array(hist)
+    extra = {}
+    if grids.nx <= 24:       # small enough to keep the final densities
+        extra = dict(rho=np.asarray(dens.rho), tau=np.asarray(dens.tau))
+    np.savez_compressed(
+        os.path.join(HERE, f"config_{name}.npz"),
+        workload=workload, maxiter=maxiter,
+        hist_iter=h[:, 0], hist_ehf=h[:, 1], hist_ehfint=h[:, 2], hist_efluct1=h[:, 3],
+        hist_efluct2=h[:, 4], hist_x0dmp=h[:, 5], hist_epair=h[:, 6],
+        sp_energy=np.asarray(levels.sp_energy), sp_kinetic=np.asarray(levels.sp_kinetic),
+        sp_norm=np.asarray(levels.sp_norm),
+        wocc=np.asarray(levels.wocc), wguv=np.asarray(levels.wguv), deltaf=np.asarray(levels.deltaf),
+        eferm=np.asarray(pairs.eferm), epair=np.asarray(pairs.epair),
+        rms=np.asarray(obs.rms), rmstot=np.asarray(obs.rmstot),
+        ehf=float(en.ehf), ehfint=float(en.ehfint),
+        nneut=levels.nneut, nprot=levels.nprot, npsi=np.asarray(levels.npsi),
+        **{f"lastdiag_{k}": v for k, v in lastd.items()}, **extra)
+    print(f"{name}: {len(hist)} energy records, ehf={en.ehf:.10f}", flush=True)
+
+
+def natural_vectors(m, ref):
+    """static.hfb_natural (configuration-space sub-iterations) on seeded
+    inputs on an 8^3 grid (3 + 2 particles in 4 + 3 states): Hermitian h and
+    gap matrices, an anti-Hermitian symcond, ascending single-particle
+    energies and random occupation weights, three sub-iterations for each
+    isospin in turn, once with state-dependent damping (e0bas = 10) and once
+    with the global one (e0bas = 0).  Pairing is off (forces.ipair = 0): with
+    it on, the reference's sub-iteration calls its single-isospin BCS solver
+    with a missing argument (static.py:988)."""
+    import jax.numpy as jnp
+    J = jnp.asarray
+    rng = np.random.default_rng(20261204)
+    n = 8
+    case = dict(grid=dict(nx=n, ny=n, nz=n, dx=0.9, dy=0.9, dz=0.9),
+                force=dict(name="SLy4", ipair=0, tbcs=False),
+                levels=dict(nneut=3, nprot=2, npsi=[4, 3]),
+                static=dict(maxiter=1, radinx=2.0, radiny=2.1, radinz=2.4, serr=1e-20, x0dmp=0.3, e0dmp=100.0),
+                mprint=1)
+    out = {}
+    for tag, e0bas in (("e0", 10.0), ("glob", 0.0)):
+        params, forces, grids, dens, mf, levels, static, coul, en, moment, pairs = _setup(m, ref, case)
+        nst, ld = levels.nstmax, max(levels.npsi)
+
+        def herm(scale):
+            a = rng.normal(size=(2, ld, ld)) + 1j * rng.normal(size=(2, ld, ld))
+            return scale * 0.5 * (a + np.conj(np.transpose(a, (0, 2, 1))))
+
+        h = herm(2.0)
+        spe = np.concatenate([np.sort(rng.uniform(-40, 5, levels.npsi[0])), np.sort(rng.uniform(-35, 8, levels.npsi[1]))])
+        for iq in range(2):
+            off = 0 if iq == 0 else levels.npsi[0]
+            for i in range(levels.npsi[iq]):
+                h[iq, i, i] = spe[off + i]
+        a = 0.3 * (rng.normal(size=(2, ld, ld)) + 1j * rng.normal(size=(2, ld, ld)))
+        sym = 0.5 * (a - np.conj(np.transpose(a, (0, 2, 1))))
+        ins = dict(psi=(rng.normal(size=(nst, 2, n, n, n)) + 1j * rng.normal(size=(nst, 2, n, n, n))) * 0.1,
+                   lagrange=(rng.normal(size=(nst, 2, n, n, n)) + 1j * rng.normal(size=(nst, 2, n, n, n))) * 0.1,
+                   hmatrix=h, gapmatrix=herm(0.5), symcond=sym, lambda_save=herm(1.0), sp_energy=spe,
+                   wocc=rng.uniform(0.0, 1.0, nst), wguv=rng.uniform(0.0, 0.5, nst),
+                   pairwg=rng.uniform(0.5, 1.0, nst), wstates=rng.uniform(0.8, 1.0, nst),
+                   deltaf=rng.uniform(0.0, 2.0, nst))
+        for k in ("psi", "lagrange", "sp_energy", "wocc", "wguv", "pairwg", "wstates", "deltaf"):
+            setattr(levels, k, J(ins[k]))
+        for k in ("hmatrix", "gapmatrix", "symcond", "lambda_save"):
+            setattr(static, k, J(ins[k]))
+        static.e0bas = e0bas
+        static.delstepbas = 2.0
+        for k, v in ins.items():
+            out[f"{tag}_in_{k}"] = np.asarray(v)
+        for iq in range(2):
+            levels, static = m["static"].hfb_natural(forces, grids, levels, mf, params, static, iq, 3)
+        for k in ("psi", "lagrange", "sp_energy", "deltaf"):
+            out[f"{tag}_out_{k}"] = np.asarray(getattr(levels, k))
+        for k in ("hmatrix", "gapmatrix", "symcond", "lambda_save"):
+            out[f"{tag}_out_{k}"] = np.asarray(getattr(static, k))
+    np.savez_compressed(os.path.join(HERE, "natural_n8.npz"), **out)
+    print("natural_n8: hfb_natural on seeded inputs", flush=True)
 
 
 def _smooth_random(rng, shape, n, scale):
@@ -388,10 +520,16 @@ def main():
         res_writer_vectors(m, a.ref)
     if a.only in (None, "constraint"):
         constraint_vectors(m, a.ref)
+    if a.only in (None, "natural"):
+        natural_vectors(m, a.ref)
     for name, case in RUN_CASES.items():
         if a.only in (None, name):
             m = _import_reference(a.ref)
             run_case(m, a.ref, name, case)
+    for name, c in CONFIG_RUNS.items():
+        if a.only in (None, "config", name):
+            m = _import_reference(a.ref)
+            config_run(m, a.ref, name, c["workload"], c["maxiter"])
 
 
 if __name__ == "__main__":

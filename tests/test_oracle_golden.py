@@ -294,3 +294,70 @@ def test_constraint_oracle_against_reference():
     assert rel(cor, z["psi_corrected"]) < 1e-13
     pot = oc.constraint_potential(np.moveaxis(z["upot_xyzs"], -1, 0), f, z["lambda1"])
     assert rel(pot, np.moveaxis(z["pot_xyzs"], -1, 0)) < 1e-14
+
+
+# ---- lastdiag on the bench workloads' final matrices --------------------
+from cases import CONFIG_RUNS  # noqa: E402
+
+
+def qp_cluster_norms(e, q, tol=1e-7):
+    """Quasiparticle norms summed in quadrature over clusters of degenerate
+    energies (Kramers pairs): the norm of one eigenvector depends on the
+    basis the eigensolver picks inside a degenerate subspace, the cluster
+    sum does not.  Returns (cluster energies, cluster norms^2)."""
+    e = np.asarray(e)
+    q = np.asarray(q)
+    ce, cq = [], []
+    i = 0
+    while i < len(e):
+        j = i + 1
+        while j < len(e) and abs(e[j] - e[i]) <= tol * max(1.0, abs(e[i])):
+            j += 1
+        ce.append(e[i])
+        cq.append(float(np.sum(q[i:j] ** 2)))
+        i = j
+    return np.array(ce), np.array(cq)
+
+
+@pytest.mark.parametrize("name", sorted(CONFIG_RUNS))
+def test_oracle_lastdiag_matches_reference(name):
+    """The restated lastdiag (reference index ranges) on the h and gap
+    matrices, occupations and Fermi energies the reference driver held at
+    its end reproduces the reference's quasiparticle energies and the
+    degenerate-cluster sums of its lower-component norms."""
+    d = np.load(os.path.join(G, f"config_{name}.npz"))
+    nneut, nprot = int(d["nneut"]), int(d["nprot"])
+    for iq in range(2):
+        nst = nneut if iq == 0 else nprot
+        start = 0 if iq == 0 else nneut
+        e, q = static.lastdiag_block(d["lastdiag_hmatrix"][iq, :nst, :nst], d["lastdiag_gapmatrix"][iq, :nst, :nst],
+                                     d["lastdiag_wocc"][start:start + nst], float(d["lastdiag_eferm"][iq]), start)
+        er, qr = d[f"lastdiag_qp_energy_{iq}"], d[f"lastdiag_qp_norm_{iq}"]
+        assert np.max(np.abs(e - er)) <= 1e-10 * max(1.0, np.max(np.abs(er)))
+        ce, cq = qp_cluster_norms(e, q)
+        cer, cqr = qp_cluster_norms(er, qr)
+        assert len(ce) == len(cer)
+        assert np.max(np.abs(cq - cqr)) <= 1e-10
+
+
+# ---- hfb_natural on seeded inputs ---------------------------------------
+@pytest.mark.parametrize("tag", ["e0", "glob"])
+def test_oracle_hfb_natural_matches_reference(tag):
+    """The restated configuration-space sub-iterations (reference index
+    ranges, pairing off) reproduce the reference's hfb_natural: rotated
+    states and Lagrange fields, transformed h and gap matrices, lambda,
+    the updated symcond and single-particle energies."""
+    import types
+    d = np.load(os.path.join(G, "natural_n8.npz"))
+    lv = types.SimpleNamespace(nneut=3, nprot=2, npsi=[4, 3], nstmax=7)
+    for k in ("psi", "lagrange", "sp_energy", "wocc", "wguv", "pairwg", "wstates", "deltaf"):
+        setattr(lv, k, d[f"{tag}_in_{k}"].copy())
+    st = types.SimpleNamespace(e0bas=10.0 if tag == "e0" else 0.0, delstepbas=2.0)
+    for k in ("hmatrix", "gapmatrix", "symcond", "lambda_save"):
+        setattr(st, k, d[f"{tag}_in_{k}"].copy())
+    for iq in range(2):
+        static.hfb_natural(lv, st, iq, 3, reference_indexing=True)
+    for k in ("psi", "lagrange", "sp_energy"):
+        assert rel(getattr(lv, k), d[f"{tag}_out_{k}"]) < 1e-12, k
+    for k in ("hmatrix", "gapmatrix", "symcond", "lambda_save"):
+        assert rel(getattr(st, k), d[f"{tag}_out_{k}"]) < 1e-12, k
