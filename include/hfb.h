@@ -291,6 +291,28 @@ int hfb_natural_symcond(hfb_ctx_t ctx, const hfb_natural_args* a, void* stream);
 int hfb_natural_end(hfb_ctx_t ctx, int prec, const hfb_natural_args* a, const void* psi, void* psi_out,
                     void* lagrange, void* stream);
 
+/* State-vector algebra for the linear-response solver of the sensitivities
+ * (no counterpart in the reference, which has no differentiation): sets of
+ * nsp two-spinors laid out like psi, precision prec.
+ *   hfb_state_dot:       *out (device double) = wxyz sum Re(conj(a) b)
+ *   hfb_state_axpby:     y = a x + b y
+ *   hfb_state_mul_field: y_s = field x_s, field [nx][ny][nz] double
+ *   hfb_state_project:   v_j -= sum_i psi_i wxyz <psi_i | v_j> (np states
+ *                        psi, nv states v; np * nv <= 10240)
+ *   hfb_state_axpby_diag: y_s = a_s x_s + b y_s, a device double[nsp]
+ *   hfb_rms_field:       field = scale (|r - cm|^2 - r0^2) on the centred
+ *                        grid (cm host double[3]): the derivative of a point
+ *                        rms radius r0 about cm with respect to the density,
+ *                        with scale = 1 / (2 N r0) */
+int hfb_state_dot(hfb_ctx_t ctx, int prec, int nsp, const void* a, const void* b, double* out, void* stream);
+int hfb_state_axpby(hfb_ctx_t ctx, int prec, int nsp, double a, const void* x, double b, void* y, void* stream);
+int hfb_state_mul_field(hfb_ctx_t ctx, int prec, int nsp, const double* field, const void* x, void* y,
+                        void* stream);
+int hfb_state_project(hfb_ctx_t ctx, int prec, int np, const void* psi, int nv, void* v, void* stream);
+int hfb_state_axpby_diag(hfb_ctx_t ctx, int prec, int nsp, const double* a, const void* x, double b, void* y,
+                         void* stream);
+int hfb_rms_field(hfb_ctx_t ctx, const double* cm, double r0, double scale, double* field, void* stream);
+
 /* ---- pairs.py ---------------------------------------------------------- */
 typedef struct hfb_pair_args {
   int npsi[2];

@@ -368,8 +368,9 @@ __device__ __forceinline__ void hb_tile(const HbArgs& a, const HbThread& t, HbSh
   if (threadIdx.x == 0) {
     tc::fence_after();
     if (!b_ready) {
-      if (!tc::mbar_wait(&sh.bar_b, 0, a.wait_limit)) sh.bad = 1;
-      b_ready = true;
+      // on a timeout b_ready stays false: the exit path waits for the copy
+      if (tc::mbar_wait(&sh.bar_b, 0, a.wait_limit)) b_ready = true;
+      else sh.bad = 1;
     }
     if (!sh.bad) {
       hb_gemm<N>(t.tb, bax, false);
@@ -608,8 +609,10 @@ __global__ void __launch_bounds__(kHbThreads, 2) hpsi_bf3_kernel(HbArgs a) {
       hb_tile<N, 1, 1>(a, t, sh, bsm, s, tile, phase, b_ready);
     else
       hb_tile<N, 0, 2>(a, t, sh, bsm, s, tile, phase, b_ready);
-    __syncthreads();   // sh.next and sh.bad are visible; the tile's accumulator reads are done
+    // every thread reads sh.next (written before the tile's first barrier)
+    // before this barrier, and thread 0 rewrites it only after it
     task = sh.next;
+    __syncthreads();   // sh.bad is visible; the tile's accumulator reads are done
   }
   tc::fence_before();
   __syncthreads();

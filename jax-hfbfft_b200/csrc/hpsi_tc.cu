@@ -426,8 +426,9 @@ __device__ __forceinline__ void ht_tile(const HtArgs& a, const HtThread& t, HtSh
   if (threadIdx.x == 0) {
     tc::fence_after();
     if (!b_ready) {
-      if (!tc::mbar_wait(&sh.bar_b, 0, kHtWaitLimit)) sh.bad = 1;
-      b_ready = true;
+      // on a timeout b_ready stays false: the exit path waits for the copy
+      if (tc::mbar_wait(&sh.bar_b, 0, kHtWaitLimit)) b_ready = true;
+      else sh.bad = 1;
     }
     ht_gemm<N>(t.tb, kD1R, kD1I, bhi, false);
     tc::mma_commit(&sh.bar_mma);

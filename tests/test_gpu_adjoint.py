@@ -1,6 +1,10 @@
-"""Energy sensitivities (hfb.adjoint) against central finite differences of
-the self-consistent binding energy, on the Ca48 sensitivity workload
-(32^3, dx 0.8 fm, 40 + 30 states, SLy4 + volume delta pairing)."""
+"""Sensitivities (hfb.adjoint) against central finite differences (relative
+step 1e-4) of the self-consistent solution, on the Ca48 sensitivity
+workload (32^3, dx 0.8 fm, 40 + 30 states, SLy4 + volume delta pairing):
+the binding energy's explicit gradient for all eleven Skyrme couplings and
+both pairing strengths, and the proton rms radius's gradient by the
+implicit adjoint (linear-response solve at the fixed point).  Ca48 is
+doubly magic: its BCS gap collapses and the occupations are 0 or 1."""
 import numpy as np
 import pytest
 import torch
@@ -21,7 +25,7 @@ def test_coupling_gradient_matches_central_fd(ca48):
     1e-4 relative for the Skyrme couplings."""
     from hfb import adjoint
     case, st = ca48
-    names = ["t0", "x1", "t3", "power", "W0"]
+    names = ["t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power"]
     g = adjoint.coupling_gradient(st)
     fd = adjoint.fd_gradient(case, names, rel_step=1e-4, base=st, tol=1e-11)
     for n in names:
@@ -36,8 +40,9 @@ def test_pairing_strength_gradient_collapsed_pairing(ca48):
     from hfb import adjoint
     case, st = ca48
     g = adjoint.coupling_gradient(st)
-    fd = adjoint.fd_gradient(case, ["v0neut"], rel_step=1e-4, base=st, tol=1e-11)
-    assert abs(g["v0neut"]) < 1e-5 and abs(fd["v0neut"]) < 1e-5
+    fd = adjoint.fd_gradient(case, ["v0neut", "v0prot"], rel_step=1e-4, base=st, tol=1e-11)
+    for n in ("v0neut", "v0prot"):
+        assert abs(g[n]) < 1e-5 and abs(fd[n]) < 1e-5
 
 
 @pytest.mark.gpu
@@ -54,3 +59,41 @@ def test_binding_energy_autograd_function(ca48):
     g = adjoint.coupling_gradient(st)
     assert abs(float(e.detach()) - st["energies"].ehf) < 1e-8
     np.testing.assert_allclose(theta.grad.numpy(), [g[n] for n in names], rtol=1e-6)
+
+
+@pytest.fixture(scope="module")
+def ca48_states():
+    """Ca48 converged until the proton rms radius itself is stationary to
+    1e-13 fm (an energy criterion leaves the states converged only to about
+    the square root of its tolerance)."""
+    from hfb import config, adjoint
+    case = config.case_dict("Ca48")
+    st, R = adjoint.converge_states(case, tol_r=1e-13)
+    return case, st
+
+
+@pytest.mark.gpu
+def test_rms_gradient_implicit_adjoint_matches_central_fd(ca48_states):
+    """dr_rms(p)/dtheta for the eleven Skyrme couplings: the adjoint solve
+    (CG on the occupied-virtual orbital Hessian) against central
+    differences of the reconverged radius, 1e-3 relative (absolute 1e-7 fm
+    per unit coupling for the near-zero ones)."""
+    from hfb import adjoint
+    case, st = ca48_states
+    names = ["t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power"]
+    g, info = adjoint.rms_gradient(st, names, tol=1e-10)
+    assert info["residual"] < 1e-10 and info["cg_iterations"] < 500
+    fd = adjoint.fd_rms_gradient(case, names, rel_step=1e-4, base=st, tol_r=1e-13)
+    th = adjoint.theta_of(st["forces"])
+    for n in names:
+        scale = abs(fd[n]) * abs(th[n])         # d r / d ln theta
+        assert abs(g[n] - fd[n]) * abs(th[n]) <= 1e-3 * scale + 1e-7, (n, g[n], fd[n])
+
+
+@pytest.mark.gpu
+def test_rms_gradient_pairing_strengths_vanish_with_collapsed_pairing(ca48_states):
+    from hfb import adjoint
+    case, st = ca48_states
+    g, _ = adjoint.rms_gradient(st, ["v0neut", "v0prot"], tol=1e-8)
+    fd = adjoint.fd_rms_gradient(case, ["v0neut"], rel_step=1e-4, base=st, tol_r=1e-13)
+    assert abs(g["v0neut"]) < 1e-9 and abs(g["v0prot"]) < 1e-9 and abs(fd["v0neut"]) < 1e-7
