@@ -98,9 +98,9 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     // single-precision hpsi kernel: HFB_HPSI_KERNEL=bf16x3 or tf32x3
     const char* h = getenv("HFB_HPSI_KERNEL");
     c->hpsi_kind = (h && strcmp(h, "bf16x3") == 0) ? 0 : 1;
-    // FP64 Gram contractions: HFB_GRAM_F64=dmma (FP64 tensor cores) or simt
-    const char* gk = getenv("HFB_GRAM_F64");
-    c->gram_f64_dmma = (gk && strcmp(gk, "dmma") == 0) ? 1 : 0;
+    // FP64 Gram and rotation on the FP64 tensor cores: HFB_F64_MMA=1
+    const char* gk = getenv("HFB_F64_MMA");
+    c->f64_mma = (gk && gk[0] == '1') ? 1 : 0;
     c->wait_limit = kDefaultWaitLimit;
     c->timeout_probe = 0;
   }

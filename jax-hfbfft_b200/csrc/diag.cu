@@ -307,7 +307,7 @@ int gram_launch(hfb_ctx_s* c, int prec, int nblk, const int* s0, const int* ns, 
   GramOut ot;
   for (int q = 0; q < 8; ++q) ot.p[q] = outs_host[q];
   dim3 grid(job.ntile, nchunk);
-  if (prec == HFB_F64 && c->gram_f64_dmma) {
+  if (prec == HFB_F64 && c->f64_mma) {
     static const bool smem_ok =
         cudaFuncSetAttribute(gram_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GD_SMEM) ==
         cudaSuccess;
@@ -1415,6 +1415,97 @@ rotate_kernel(int ns, size_t K, const cplx<R>* __restrict__ psi, const double2* 
   }
 }
 
+// FP64 states on the FP64 tensor cores (mma.sync m8n8k4 .f64): with the
+// state index interleaved with (Re, Im), i' = 2 i + part,
+//   A'[k][i'] = (Re, Im) psi_i(k),
+//   Re out_j(k) = sum_i' A'[k][i'] Br[i'][j],  Br = (Re W_ij, -Im W_ij),
+//   Im out_j(k) = sum_i' A'[k][i'] Bi[i'][j],  Bi = (Im W_ij,  Re W_ij),
+// W = [U | L].  A CTA (8 warps, 4 along k x 2 along j, 32 x 32 outputs
+// per warp, 4 x 4 MMA blocks) computes 128 grid points x 64 outputs,
+// streaming the states in double-buffered stages of 4.
+constexpr int RD_KT = 128, RD_JT = 64, RD_IT = 4;
+
+__global__ void __launch_bounds__(256) rotate_dmma_kernel(int ns, size_t K, const double2* __restrict__ psi,
+                                                          const double2* __restrict__ U,
+                                                          const double2* __restrict__ L, int ld, double2* out1,
+                                                          double2* out2) {
+  __shared__ double2 Ps[2][RD_IT][RD_KT + 1];
+  __shared__ double2 Ws[2][RD_IT][RD_JT + 1];
+  const int njt = (2 * ns + RD_JT - 1) / RD_JT;
+  const int jt = blockIdx.x % njt;
+  const size_t k0 = (size_t)(blockIdx.x / njt) * RD_KT;
+  const int j0 = jt * RD_JT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wk = warp & 3, wj = warp >> 2;
+  const int fr = lane >> 2, fk = lane & 3;
+  double accR[4][4][2], accI[4][4][2];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) accR[u][v][0] = accR[u][v][1] = accI[u][v][0] = accI[u][v][1] = 0.0;
+  auto load = [&](int buf, int i0) {
+    for (int e = threadIdx.x; e < RD_IT * RD_KT; e += 256) {
+      const int ii = e / RD_KT, kk = e % RD_KT;
+      const size_t k = k0 + kk;
+      Ps[buf][ii][kk] = (i0 + ii < ns && k < K) ? psi[(size_t)(i0 + ii) * K + k] : make_double2(0.0, 0.0);
+    }
+    for (int e = threadIdx.x; e < RD_IT * RD_JT; e += 256) {
+      const int ii = e / RD_JT, jj = e % RD_JT;
+      const int j = j0 + jj;
+      double2 w = make_double2(0.0, 0.0);
+      if (i0 + ii < ns && j < 2 * ns)
+        w = j < ns ? U[(size_t)(i0 + ii) * ld + j] : L[(size_t)(i0 + ii) * ld + (j - ns)];
+      Ws[buf][ii][jj] = w;
+    }
+  };
+  load(0, 0);
+  __syncthreads();
+  int buf = 0;
+  for (int i0 = 0; i0 < ns; i0 += RD_IT) {
+    if (i0 + RD_IT < ns) load(buf ^ 1, i0 + RD_IT);
+#pragma unroll
+    for (int kk = 0; kk < RD_IT / 2; ++kk) {
+      const int ii = 2 * kk + (fk >> 1);     // state of this lane's k' within the step
+      const bool im = fk & 1;
+      double a[4], br[4], bi[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double2 p = Ps[buf][ii][32 * wk + 8 * u + fr];
+        a[u] = im ? p.y : p.x;
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const double2 w = Ws[buf][ii][32 * wj + 8 * v + fr];
+        br[v] = im ? -w.y : w.x;
+        bi[v] = im ? w.x : w.y;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          gd_mma(accR[u][v], a[u], br[v]);
+          gd_mma(accI[u][v], a[u], bi[v]);
+        }
+    }
+    __syncthreads();
+    buf ^= 1;
+  }
+  // the thread holds rows k = 32 wk + 8 u + fr, columns j = 32 wj + 8 v + 2 fk + c
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int c2 = 0; c2 < 2; ++c2) {
+      const int j = j0 + 32 * wj + 8 * v + 2 * fk + c2;
+      if (j >= 2 * ns) continue;
+      double2* o = j < ns ? out1 + (size_t)j * K : out2 + (size_t)(j - ns) * K;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const size_t k = k0 + 32 * wk + 8 * u + fr;
+        if (k < K) o[k] = make_double2(accR[u][v][c2], accI[u][v][c2]);
+      }
+    }
+}
+
 // Single-precision variant with a larger register tile: 128 (k) x 96 (j)
 // per CTA, 256 threads holding 8 x 6 complex accumulators each (48
 // independent chains), 8 states per double-buffered shared-memory stage.
@@ -1532,7 +1623,12 @@ int rotate_launch(hfb_ctx_s* c, int prec, int s0, int ns, const void* psi, const
   const int njt = (2 * ns + 63) / 64;
   const size_t nkt = (K + 63) / 64;
   const size_t off = (size_t)s0 * K;
-  if (prec == HFB_F64)
+  if (prec == HFB_F64 && c->f64_mma) {
+    const int njd = (2 * ns + RD_JT - 1) / RD_JT;
+    const size_t nkd = (K + RD_KT - 1) / RD_KT;
+    rotate_dmma_kernel<<<(unsigned)(nkd * njd), 256, 0, st>>>(ns, K, (const double2*)psi + off, U, L, ld,
+                                                             (double2*)out1 + off, (double2*)out2 + off);
+  } else if (prec == HFB_F64)
     rotate_kernel<double><<<(unsigned)(nkt * njt), 256, 0, st>>>(ns, K, (const double2*)psi + off, U, L, ld,
                                                                  (double2*)out1 + off, (double2*)out2 + off);
   else {
