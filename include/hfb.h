@@ -180,6 +180,10 @@ typedef struct hfb_grstep_args {
   double* sp_efluct1;      /* in/out                                         */
   double* sp_efluct2;      /* in/out                                         */
   double* sums;            /* out [2]: sum(sp_efluct1), sum(wocc*wstates*denerg) */
+  const double* x0dmp_dev; /* optional: a device double read in place of
+                              x0dmp (the step size kept on the device by
+                              hfb_step_control, so that iterations can be
+                              replayed without the host)                  */
 } hfb_grstep_args;
 /* grstep (static.py:215-259) with grstep_helper / e0dmp_gt_zero / laplace. */
 int hfb_grstep(hfb_ctx_t ctx, int prec, const hfb_grstep_args* a, void* stream);
@@ -312,6 +316,17 @@ int hfb_state_project(hfb_ctx_t ctx, int prec, int np, const void* psi, int nv, 
 int hfb_state_axpby_diag(hfb_ctx_t ctx, int prec, int nsp, const double* a, const void* x, double b, void* y,
                          void* stream);
 int hfb_rms_field(hfb_ctx_t ctx, const double* cm, double r0, double scale, double* field, void* stream);
+
+/* Step-size control and energy history on the device (the host loop of
+ * static.py:1864-1878 moved to one device thread, so that iterations can be
+ * replayed without host reads in between; no counterpart in the
+ * reference).  After an iteration's energies: hist[*count] = *ehf and
+ * *count += 1 while *count < max_hist; with ctl[5] != 0 the reference's
+ * adaptation of the step size ctl[0] from E_bind and efluct (device double
+ * [4]: efluct1 of each isospin, efluct2 of each isospin), with ctl[1..3] the
+ * previous E_bind, efluct1, efluct2 and ctl[4] the minimum step. */
+int hfb_step_control(hfb_ctx_t ctx, const double* ehf, const double* efluct, double* ctl, double* hist,
+                     int* count, int max_hist, void* stream);
 
 /* ---- pairs.py ---------------------------------------------------------- */
 typedef struct hfb_pair_args {

@@ -208,7 +208,7 @@ precond_b_kernel(cplx<R>* tmp, int nneut, const double* __restrict__ wg, const d
 // C: x-plane, inverse along y and z, then write or update.
 template <class R, int N>
 __global__ void __launch_bounds__(PlaneGeo<R, N>::THREADS)
-precond_c_kernel(const cplx<R>* tmp, int mode, double x0, cplx<R>* dst) {
+precond_c_kernel(const cplx<R>* tmp, int mode, double x0, const double* x0_dev, cplx<R>* dst) {
   using G = PlaneGeo<R, N>;
   using Z = cplx<R>;
   constexpr size_t N2 = (size_t)N * N, N3 = N2 * N;
@@ -232,7 +232,7 @@ precond_c_kernel(const cplx<R>* tmp, int mode, double x0, cplx<R>* dst) {
   __syncthreads();
   for (int c = 0; c < 2; ++c) plane_lines<R, N, true, +1>(plane + c * N * G::LD, xb, tw, line, p, active);
   __syncthreads();
-  const R xr = (R)x0;
+  const R xr = (R)(x0_dev ? *x0_dev : x0);
   for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
     int c = e / (N * N), r = e - c * N * N;
     size_t g = off + (size_t)c * N3 + r;
@@ -246,7 +246,7 @@ template <class R, int N>
 int precond_launch_t(hfb_ctx_s* c, int ns, int nneut, const void* src, const void* lag, int use_lag, const void* psi,
                      const double* coef, const double* wg, const double* wu, const double* vmax_dev, double vmax_host,
                      double e0, double h2ma, int mode, double x0, void* tmp, void* dst, double* fluct,
-                     cudaStream_t st) {
+                     cudaStream_t st, const double* x0_dev) {
   using G = PlaneGeo<R, N>;
   using Z = cplx<R>;
   if (ns <= 0) return HFB_OK;
@@ -261,7 +261,7 @@ int precond_launch_t(hfb_ctx_s* c, int ns, int nneut, const void* src, const voi
   precond_b_kernel<R, N><<<grid, G::THREADS, G::SMEM, st>>>((Z*)tmp, nneut, wg, wu, vmax_dev, vmax_host, e0, h2ma,
                                                             kf[0], kf[1], kf[2]);
   HFB_CHECK_LAUNCH();
-  precond_c_kernel<R, N><<<grid, G::THREADS, G::SMEM, st>>>((const Z*)tmp, mode, x0, (Z*)dst);
+  precond_c_kernel<R, N><<<grid, G::THREADS, G::SMEM, st>>>((const Z*)tmp, mode, x0, x0_dev, (Z*)dst);
   HFB_CHECK_LAUNCH();
   return HFB_OK;
 }
@@ -269,14 +269,14 @@ int precond_launch_t(hfb_ctx_s* c, int ns, int nneut, const void* src, const voi
 int precond_launch(hfb_ctx_s* c, int prec, int ns, int nneut, const void* src, const void* lag, int use_lag,
                    const void* psi, const double* coef, const double* wg, const double* wu, const double* vmax_dev,
                    double vmax_host, double e0, double h2ma, int mode, double x0, void* tmp, void* dst,
-                   double* fluct, cudaStream_t st) {
+                   double* fluct, cudaStream_t st, const double* x0_dev) {
   return dispatch_n(c->n, [&](auto nn) -> int {
     constexpr int N = decltype(nn)::value;
     if (prec == HFB_F64)
       return precond_launch_t<double, N>(c, ns, nneut, src, lag, use_lag, psi, coef, wg, wu, vmax_dev, vmax_host, e0,
-                                         h2ma, mode, x0, tmp, dst, fluct, st);
+                                         h2ma, mode, x0, tmp, dst, fluct, st, x0_dev);
     return precond_launch_t<float, N>(c, ns, nneut, src, lag, use_lag, psi, coef, wg, wu, vmax_dev, vmax_host, e0,
-                                      h2ma, mode, x0, tmp, dst, fluct, st);
+                                      h2ma, mode, x0, tmp, dst, fluct, st, x0_dev);
   });
 }
 
@@ -326,11 +326,12 @@ __global__ void state_reduce_kernel(int ns, int nplanes, const double* part, int
 
 // Simple damped step when e0dmp <= 0 (static.py:181-185).
 template <class R>
-__global__ void simple_step_kernel(int ns, size_t n3, const double* spe_new, const double* spe_old, double x0,
-                                   const cplx<R>* ps1, cplx<R>* psi) {
+__global__ void simple_step_kernel(int ns, size_t n3, const double* spe_new, const double* spe_old, double x0h,
+                                   const double* x0_dev, const cplx<R>* ps1, cplx<R>* psi) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   size_t tot = (size_t)ns * 2 * n3;
   if (i >= tot) return;
+  const double x0 = x0_dev ? *x0_dev : x0h;
   int s = (int)(i / (2 * n3));
   R a = (R)(1.0 + x0 * (spe_new[s] - spe_old[s]));
   psi[i] = a * psi[i] - (R)x0 * ps1[i];
@@ -408,16 +409,17 @@ extern "C" int hfb_grstep(hfb_ctx_t ctx, int prec, const hfb_grstep_args* a, voi
   // 2) damped step
   if (a->e0dmp > 0.0) {
     r = precond_launch(ctx, prec, ns, a->nneut, a->hmfpsi, a->lagrange, a->use_lagrange, a->psi, hexp, lw, lu, vmax,
-                       0.0, a->e0dmp, a->h2ma, 1, a->x0dmp, a->hmfpsi, a->psi, a->do_fluct ? fl : nullptr, st);
+                       0.0, a->e0dmp, a->h2ma, 1, a->x0dmp, a->hmfpsi, a->psi, a->do_fluct ? fl : nullptr, st,
+                       a->x0dmp_dev);
     if (r) return r;
   } else {
     size_t tot = (size_t)ns * 2 * n3;
     if (prec == HFB_F64)
       simple_step_kernel<double><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(
-          ns, n3, spe_new, a->sp_energy, a->x0dmp, (const double2*)a->hmfpsi, (double2*)a->psi);
+          ns, n3, spe_new, a->sp_energy, a->x0dmp, a->x0dmp_dev, (const double2*)a->hmfpsi, (double2*)a->psi);
     else
       simple_step_kernel<float><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(
-          ns, n3, spe_new, a->sp_energy, a->x0dmp, (const float2*)a->hmfpsi, (float2*)a->psi);
+          ns, n3, spe_new, a->sp_energy, a->x0dmp, a->x0dmp_dev, (const float2*)a->hmfpsi, (float2*)a->psi);
     HFB_CHECK_LAUNCH();
   }
   grstep_finish_kernel<<<1, 256, 0, st>>>(ns, a->do_fluct && a->e0dmp > 0.0, n, fl, a->wxyz, spe_new, a->wocc,

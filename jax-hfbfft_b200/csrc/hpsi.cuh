@@ -36,7 +36,8 @@ int hpsi_ovl_parts(hfb_ctx_s* c, int prec);
 //  v = src - (use_lag ? lag : coef[s] * psi)     (plain src if psi == NULL)
 //  out = F^-1[ F[v] / (denom(k) * Ntot) ]       (unnormalised transforms)
 //  mode 0: dst = out;  mode 1: dst -= x0 * out   (dst = psi in the gradient step)
-// ``tmp`` holds the intermediate spectrum (may alias src or dst).
+// ``tmp`` holds the intermediate spectrum (may alias src or dst).  ``x0_dev``
+// (optional) is a device double read in place of x0.
 // ``fluct`` (optional) receives per-(state, x-plane) partial sums [ns][n][2]
 // of |v|^2 and |lag - coef psi|^2.  ``wg``, ``wu`` are per-state weights
 // before the max(., 0.1) floor; the pairing shift uses vmax_dev[iq] when
@@ -44,6 +45,6 @@ int hpsi_ovl_parts(hfb_ctx_s* c, int prec);
 int precond_launch(hfb_ctx_s* c, int prec, int ns, int nneut, const void* src, const void* lag, int use_lag,
                    const void* psi, const double* coef, const double* wg, const double* wu, const double* vmax_dev,
                    double vmax_host, double e0, double h2ma, int mode, double x0, void* tmp, void* dst,
-                   double* fluct, cudaStream_t st);
+                   double* fluct, cudaStream_t st, const double* x0_dev = nullptr);
 
 }  // namespace hfb

@@ -45,7 +45,7 @@ class GrstepArgs(C.Structure):
                 ("x0dmp", C.c_double), ("e0dmp", C.c_double), ("h2ma", C.c_double), ("wxyz", C.c_double),
                 ("pot", vp), ("v_pair", vp), ("psi", vp), ("hampsi", vp), ("hmfpsi", vp), ("delpsi", vp),
                 ("lagrange", vp), ("wocc", vp), ("wguv", vp), ("pairwg", vp), ("wstates", vp),
-                ("sp_energy", vp), ("sp_efluct1", vp), ("sp_efluct2", vp), ("sums", vp)]
+                ("sp_energy", vp), ("sp_efluct1", vp), ("sp_efluct2", vp), ("sums", vp), ("x0dmp_dev", vp)]
 
 
 class DiagArgs(C.Structure):
@@ -98,6 +98,7 @@ _PROTOS = {
     "hfb_pair": [vp, C.POINTER(PairArgs), vp],
     "hfb_lastdiag": [vp, C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, vp],
     "hfb_natural_begin": [vp, C.POINTER(NaturalArgs), vp],
+    "hfb_step_control": [vp, vp, vp, vp, vp, vp, C.c_int, vp],
     "hfb_state_dot": [vp, C.c_int, C.c_int, vp, vp, vp, vp],
     "hfb_state_axpby": [vp, C.c_int, C.c_int, C.c_double, vp, C.c_double, vp, vp],
     "hfb_state_mul_field": [vp, C.c_int, C.c_int, vp, vp, vp, vp],

@@ -9,11 +9,16 @@ refinement) on a CUDA stream of its own; a pool of host threads keeps
 different nuclei overlap on the GPU.  Instances share nothing on the
 device, so each result is the one the instance gives alone.
 
+``run_sweep_graph`` instead advances a group of instances together: after
+their start-up iterations, blocks of iterations of every instance in the
+group are captured into one CUDA graph (hfb.graph) and each graph launch
+runs them all, with the host reading the energies once per block.
+
 ``sweep_cases`` draws the instances of the sweep workload: species uniform
 over SPECIES and each coupling (t0-t3, x0-x3, W0; W0 moves b4p with it)
 scaled by an independent uniform factor in [1 - rel, 1 + rel].
 
-    python -m hfb.batch [--instances 256] [--workers 16] [--seed 20261203]
+    python -m hfb.batch [--instances 256] [--workers 16] [--seed 20261203] [--graph --group 32]
 """
 import argparse
 import json
@@ -99,23 +104,47 @@ def run_sweep(cases, workers=8, maxiter=1500):
         return list(ex.map(job, range(len(cases))))
 
 
+def run_sweep_graph(cases, group=32, maxiter=1500, block=10):
+    """Solve every case with the graph driver, ``group`` instances per
+    graph (the groups one after the other).  Results in case order."""
+    from . import graph
+    out = []
+    for g0 in range(0, len(cases), group):
+        chunk = cases[g0:g0 + group]
+        t0 = time.perf_counter()
+        states = [config.setup(c[1], dtype=torch.complex64) for c in chunk]
+        res = graph.solve(states, maxiter=maxiter, block=block)
+        dt = time.perf_counter() - t0
+        for c, r in zip(chunk, res):
+            out.append(dict(species=c[0], ehf=r["E"][-1], iterations=r["iterations"],
+                            switch_iteration=r["switch"], seconds=dt))
+        del states, res
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m hfb.batch")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--maxiter", type=int, default=1500)
+    ap.add_argument("--graph", action="store_true", help="graph driver: groups of instances per CUDA graph")
+    ap.add_argument("--group", type=int, default=32)
     args = ap.parse_args(argv)
     cases = sweep_cases(args.instances, args.seed)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    res = run_sweep(cases, workers=args.workers, maxiter=args.maxiter)
+    if args.graph:
+        res = run_sweep_graph(cases, group=args.group, maxiter=args.maxiter)
+    else:
+        res = run_sweep(cases, workers=args.workers, maxiter=args.maxiter)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     counts = {}
     for r in res:
         counts[r["species"]] = counts.get(r["species"], 0) + 1
-    print(json.dumps(dict(op="sweep", instances=len(res), workers=args.workers, seconds=dt,
+    print(json.dumps(dict(op="sweep", instances=len(res), workers=args.workers, graph=args.graph,
+                          group=args.group if args.graph else None, seconds=dt,
                           instances_per_second=len(res) / dt, species=counts,
                           iterations=int(sum(r["iterations"] for r in res)))), flush=True)
 

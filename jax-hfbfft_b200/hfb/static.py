@@ -131,6 +131,8 @@ def grstep(forces, grids, levels, meanfield, params, static):
     a.sp_energy, a.sp_efluct1, a.sp_efluct2 = ptr(lv.sp_energy), ptr(lv.sp_efluct1), ptr(lv.sp_efluct2)
     sums = static.sums_dev[2:4]
     a.sums = ptr(sums)
+    x0d = getattr(static, "x0_dev", None)       # step size kept on the device (graph replays)
+    a.x0dmp_dev = ptr(x0d) if x0d is not None else None
     call("hfb_grstep", grids.ctx.handle, prec_of(lv.psi), a, stream_ptr())
     static.sums_dev[0:2] += sums
     # delpsi = v_pair * psi_new (static.py:203, 250): diagstep forms it on the fly
@@ -282,12 +284,13 @@ def prepare(coulomb, densities, energies, forces, grids, levels, meanfield, para
     return energies
 
 
-def iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs,
-            x0_schedule=None):
-    """One pass of the loop body (static.py:1755-1882).  Returns True once
-    efluct1 < serr.  ``x0_schedule[k]`` (optional) forces the step size of
-    iteration k (the reference's adaptation compares max|lambda_asym|, which
-    depends on the eigenvector basis inside degenerate subspaces)."""
+def iterate_device(i, coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs):
+    """The device work of one pass of the loop body (static.py:1755-1862):
+    gradient step, diagonalisation, BCS, densities with mixing, mean field,
+    energies -- no read back to the host.  Host decisions that depend on
+    ``i`` (BCS / diagonalisation phases, the constant gap up to iteration
+    10) are taken here, so a replay of captured iterations is only valid
+    past those phases."""
     params.iteration = i
     forces.tbcs = True if i <= static.inibcs else static._tbcssav
     static.tdiag = not (i > static.inidiag)
@@ -317,6 +320,15 @@ def iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, p
     skyrme(coulomb, densities, forces, grids, meanfield, params, static, constraints=_active_constraints(static),
            dtype=levels.psi.dtype)
     _energies(coulomb, densities, energies, forces, grids, levels, meanfield, params, pairs)
+
+
+def iterate(i, coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs,
+            x0_schedule=None):
+    """One pass of the loop body (static.py:1755-1882).  Returns True once
+    efluct1 < serr.  ``x0_schedule[k]`` (optional) forces the step size of
+    iteration k (the reference's adaptation compares max|lambda_asym|, which
+    depends on the eigenvector basis inside degenerate subspaces)."""
+    iterate_device(i, coulomb, densities, energies, forces, grids, levels, meanfield, params, static, pairs)
     energies.sync()
     grids.ctx.check(f"iteration {i}")
     en = energies
