@@ -83,6 +83,13 @@ int hfb_device_status(hfb_ctx_t ctx, void* stream, int* status_out);
  * for its own MMAs, releases its tensor memory and returns, and the context
  * stays usable.  No counterpart in the reference (JAX has no device waits). */
 int hfb_set_wait_limit(hfb_ctx_t ctx, long long cycles);
+/* Single-precision hpsi kernel of this context: 0 bf16 three-term operands
+ * on the tensor cores (two CTAs per SM), 1 tf32 three-term operands on the
+ * tensor cores, 2 FFT line transforms on CUDA cores.  Grids the tensor-core
+ * kernels do not serve (n < 24) always use 2.  Read at each launch; for an
+ * autotuner choosing per grid and state count (no counterpart in the
+ * reference). */
+int hfb_set_hpsi_kernel(hfb_ctx_t ctx, int kind);
 /* For tests of that path: the next single-precision tensor-core hpsi launch
  * on this context has its first CTA wait, before it takes any work, on a
  * device word nothing writes, so the wait runs out after the wait limit and

@@ -195,6 +195,12 @@ extern "C" int hfb_set_wait_limit(hfb_ctx_t c, long long cycles) {
   return HFB_OK;
 }
 
+extern "C" int hfb_set_hpsi_kernel(hfb_ctx_t c, int kind) {
+  if (!c || kind < 0 || kind > 2) return HFB_ERR_ARG;
+  c->hpsi_kind = kind;
+  return HFB_OK;
+}
+
 extern "C" int hfb_arm_timeout_probe(hfb_ctx_t c) {
   if (!c) return HFB_ERR_ARG;
   c->timeout_probe = 1;

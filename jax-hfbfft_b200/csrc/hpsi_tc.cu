@@ -818,7 +818,9 @@ int hpsi_tc_prepare(hfb_ctx_s* c) {
   }
 }
 
-bool hpsi_tc_available(hfb_ctx_s* c, int prec) { return prec == HFB_F32 && c->use_tcgen05 && c->hpsi_b; }
+bool hpsi_tc_available(hfb_ctx_s* c, int prec) {
+  return prec == HFB_F32 && c->use_tcgen05 && c->hpsi_kind != 2 && c->hpsi_b;
+}
 
 int hpsi_tc_parts(hfb_ctx_s* c) { return c->n * c->n / kHtLines; }
 

@@ -80,6 +80,7 @@ _PROTOS = {
     "hfb_device_status": [vp, vp, C.POINTER(C.c_int)],
     "hfb_set_wait_limit": [vp, C.c_longlong],
     "hfb_arm_timeout_probe": [vp],
+    "hfb_set_hpsi_kernel": [vp, C.c_int],
     "hfb_cderv": [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
     "hfb_laplace": [vp, C.c_int, C.c_int, vp, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp],
     "hfb_hpsi": [vp, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp],

@@ -150,7 +150,7 @@ class BatchGraph:
 
 
 def solve(states, switch_mev=5e-4, stop_mev=5e-5, floor_mev=5e-5, maxiter=4000, block=10, graph_min=60,
-          on_block=None):
+          on_block=None, tune=True):
     """Mixed-precision solves of several instances (states with complex64
     psi from hfb.config.setup) advanced together: ordinary iterations
     through the start-up phases, then graph replays of ``block`` iterations
@@ -158,12 +158,18 @@ def solve(states, switch_mev=5e-4, stop_mev=5e-5, floor_mev=5e-5, maxiter=4000, 
     precision rule of hfb.static.statichf_mixed (FP32 until the estimated
     remaining change is below ``switch_mev`` or the FP32 noise floor is
     reached, then FP64 until it is below ``stop_mev``); the graph is
-    recaptured whenever an instance switches or finishes.  Returns one dict
-    per instance: energies, the precision switch iteration, iterations."""
+    recaptured whenever an instance switches or finishes.  With ``tune``
+    the single-precision hpsi kernel of each instance is chosen by
+    measurement (hfb.tune, cached per grid and state count).  Returns one
+    dict per instance: energies, the precision switch iteration, iterations
+    and the hpsi kernel used."""
+    from . import tune as _tune
     runs = [GraphRun(s) for s in states]
-    info = [dict(switch=None, done=False, prec="f32") for _ in runs]
-    for r in runs:
+    info = [dict(switch=None, done=False, prec="f32", hpsi=None) for _ in runs]
+    for r, inf in zip(runs, info):
         r.start()
+        if tune:
+            inf["hpsi"] = _tune.tune_hpsi(r.st)
         r.plain(max(r.steady_from(), 2))
     active = list(range(len(runs)))
     tail_start = [None] * len(runs)
@@ -197,4 +203,5 @@ def solve(states, switch_mev=5e-4, stop_mev=5e-5, floor_mev=5e-5, maxiter=4000, 
                 # the FP64 arrays are new: ordinary iterations grow the
                 # library's scratch for them before the next capture
                 r.plain(2)
-    return [dict(E=r.E, switch=inf["switch"], iterations=r.i, state=r.st) for r, inf in zip(runs, info)]
+    return [dict(E=r.E, switch=inf["switch"], iterations=r.i, state=r.st, hpsi=inf["hpsi"])
+            for r, inf in zip(runs, info)]

@@ -77,3 +77,15 @@ def test_graph_solve_mixed_precision_converges_like_the_host_driver():
     res = graph.solve([config.setup(copy.deepcopy(case), dtype=torch.complex64)], stop_mev=5e-6, maxiter=3000)
     assert res[0]["switch"] is not None
     assert abs(res[0]["E"][-1] - hist[-1][1]) < 1e-3
+
+
+def test_hpsi_tuner_times_every_kernel_and_caches_the_choice():
+    from hfb import config, static, tune
+    st = config.setup(_case(24), dtype=torch.complex64)
+    static.prepare(**{k: st[k] for k in static._STATE_KEYS})
+    best = tune.tune_hpsi(st)
+    assert best in tune.KINDS.values()
+    (entry,) = [v for k, v in tune.cache().items() if k.startswith("n24_")]
+    assert set(entry["seconds"]) == set(tune.KINDS.values()) and min(entry["seconds"].values()) > 0
+    assert entry["best"] == min(entry["seconds"], key=entry["seconds"].get)
+    assert tune.tune_hpsi(st) == best      # from the cache
