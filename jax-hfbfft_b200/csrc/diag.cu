@@ -25,7 +25,7 @@ namespace hfb {
 // (140 -> 144, 96 -> 96); 192 threads (16 x 12) hold 4 x 3 outputs each.
 constexpr int GT = 48;        // tile edge (states)
 constexpr int GKS = 8;        // k per shared-memory stage
-constexpr int GCHUNK = 8192;  // k per split-K chunk
+constexpr int GCHUNK = 8192;  // k per split-K chunk (at most; shorter when the grid would be small)
 constexpr int GTHREADS = 192;
 constexpr int kGramMaxTiles = 160;
 
@@ -43,7 +43,7 @@ struct GramJob {
 template <class R>
 __global__ void __launch_bounds__(GTHREADS)
 gram_kernel(GramJob job, size_t K, size_t n3, const cplx<R>* __restrict__ psi, const cplx<R>* __restrict__ hampsi,
-            const cplx<R>* __restrict__ hmfpsi, double2* part, int nchunk) {
+            const cplx<R>* __restrict__ hmfpsi, double2* part, int nchunk, int kchunk) {
   using Z = cplx<R>;
   __shared__ Z As[2][GKS][GT + 1];
   __shared__ Z Bs[2][GKS][GT + 1];
@@ -54,8 +54,8 @@ gram_kernel(GramJob job, size_t K, size_t n3, const cplx<R>* __restrict__ psi, c
   const cplx<R>* P = psi + (size_t)job.s0[b] * K;
   const cplx<R>* X = am == 1 ? hampsi + (size_t)job.s0[b] * K : am == 2 ? hmfpsi + (size_t)job.s0[b] * K : P;
   const double* vp = job.vp[b];
-  const size_t k0 = (size_t)blockIdx.y * GCHUNK;
-  const size_t k1 = min(K, k0 + GCHUNK);
+  const size_t k0 = (size_t)blockIdx.y * kchunk;
+  const size_t k1 = min(K, k0 + (size_t)kchunk);
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;   // rows ty + 12 u, columns tx + 16 v
   R acc[4][3][2];
 #pragma unroll
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(GD_THREADS) gram_dmma_kernel(GramJob job, size
                                                                 const double2* __restrict__ psi,
                                                                 const double2* __restrict__ hampsi,
                                                                 const double2* __restrict__ hmfpsi, double2* part,
-                                                                int nchunk) {
+                                                                int nchunk, int kchunk) {
   extern __shared__ double2 gd_smem[];
   double2* As = gd_smem;                 // [2][GT][GD_LD]
   double2* Bs = gd_smem + 2 * GT * GD_LD;
@@ -154,8 +154,8 @@ __global__ void __launch_bounds__(GD_THREADS) gram_dmma_kernel(GramJob job, size
   const double2* P = psi + (size_t)job.s0[b] * K;
   const double2* X = am == 1 ? hampsi + (size_t)job.s0[b] * K : am == 2 ? hmfpsi + (size_t)job.s0[b] * K : P;
   const double* vp = job.vp[b];
-  const size_t k0 = (size_t)blockIdx.y * GCHUNK;
-  const size_t k1 = min(K, k0 + GCHUNK);
+  const size_t k0 = (size_t)blockIdx.y * kchunk;
+  const size_t k1 = min(K, k0 + (size_t)kchunk);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int rw = warp >> 1, cw = warp & 1;
   const int fr = lane >> 2, fk = lane & 3;   // fragment row (A) / column (B), k' within the 4
@@ -283,7 +283,7 @@ int gram_launch(hfb_ctx_s* c, int prec, int nblk, const int* s0, const int* ns, 
     if (r != HFB_ERR_UNSUPPORTED_GRID) return r;
   }
   const size_t n3 = (size_t)c->n * c->n * c->n, K = 2 * n3;
-  const int nchunk = (int)((K + GCHUNK - 1) / GCHUNK);
+  int kchunk = GCHUNK;   // set below from the tile count
   GramJob job{};
   job.herm_mask = 1 | 4 | 8;
   for (int b = 0; b < nblk; ++b) {
@@ -302,6 +302,18 @@ int gram_launch(hfb_ctx_s* c, int prec, int nblk, const int* s0, const int* ns, 
     }
   }
   if (job.ntile == 0) return HFB_OK;
+  // split K so that the grid has about two CTAs per SM even for few tiles
+  // and short K (small grids): chunks a multiple of 64 elements, at most
+  // GCHUNK
+  {
+    const size_t want = (size_t)(2 * 148 + job.ntile - 1) / job.ntile;
+    size_t kc = (K + want - 1) / want;
+    kc = (kc + 63) / 64 * 64;
+    if (kc < 256) kc = 256;
+    if (kc > (size_t)GCHUNK) kc = GCHUNK;
+    kchunk = (int)kc;
+  }
+  const int nchunk = (int)((K + kchunk - 1) / kchunk);
   double2* part = (double2*)scratch(c, hfb_ctx_s::S_GRAM, sizeof(double2) * (size_t)job.ntile * nchunk * GT * GT);
   if (!part) return HFB_ERR_ALLOC;
   GramOut ot;
@@ -313,13 +325,13 @@ int gram_launch(hfb_ctx_s* c, int prec, int nblk, const int* s0, const int* ns, 
         cudaSuccess;
     if (!smem_ok) return HFB_ERR_CUDA;
     gram_dmma_kernel<<<grid, GD_THREADS, GD_SMEM, st>>>(job, K, n3, (const double2*)psi, (const double2*)hampsi,
-                                                     (const double2*)hmfpsi, part, nchunk);
+                                                     (const double2*)hmfpsi, part, nchunk, kchunk);
   } else if (prec == HFB_F64)
     gram_kernel<double><<<grid, GTHREADS, 0, st>>>(job, K, n3, (const double2*)psi, (const double2*)hampsi,
-                                              (const double2*)hmfpsi, part, nchunk);
+                                              (const double2*)hmfpsi, part, nchunk, kchunk);
   else
     gram_kernel<float><<<grid, GTHREADS, 0, st>>>(job, K, n3, (const float2*)psi, (const float2*)hampsi,
-                                             (const float2*)hmfpsi, part, nchunk);
+                                             (const float2*)hmfpsi, part, nchunk, kchunk);
   HFB_CHECK_LAUNCH();
   dim3 g2((GT * GT + 255) / 256, job.ntile);
   gram_reduce_kernel<<<g2, 256, 0, st>>>(job, nchunk, part, wxyz, ot, ldo);
