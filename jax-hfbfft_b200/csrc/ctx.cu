@@ -95,12 +95,12 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     c->use_tcgen05 = (e && e[0] == '1') ? 0 : 1;
     const char* j = getenv("HFB_LAMBDA_JACOBI");
     c->lambda_refine = (j && j[0] == '1') ? 0 : 1;
-    // single-precision hpsi kernel: HFB_HPSI_KERNEL=bf16x3 or tf32x3
+    // single-precision hpsi kernel: bf16x3 (default), tf32x3 or fft (HFB_HPSI_KERNEL)
     const char* h = getenv("HFB_HPSI_KERNEL");
-    c->hpsi_kind = (h && strcmp(h, "bf16x3") == 0) ? 0 : 1;
-    // FP64 Gram and rotation on the FP64 tensor cores: HFB_F64_MMA=1
+    c->hpsi_kind = (h && strcmp(h, "tf32x3") == 0) ? 1 : (h && strcmp(h, "fft") == 0) ? 2 : 0;
+    // FP64 Gram and rotation on the FP64 tensor cores unless HFB_F64_MMA=0
     const char* gk = getenv("HFB_F64_MMA");
-    c->f64_mma = (gk && gk[0] == '1') ? 1 : 0;
+    c->f64_mma = (gk && gk[0] == '0') ? 0 : 1;
     c->wait_limit = kDefaultWaitLimit;
     c->timeout_probe = 0;
   }

@@ -24,9 +24,9 @@ struct hfb_ctx_s {
   cudaEvent_t ev_fork, ev_join;
   unsigned char* hpsi_b; // single-precision hpsi (tf32 kernel): derivative matrices in the tensor-core tile layout
   unsigned char* hpsi_bf3_b; // single-precision hpsi (bf16 three-term kernel): the same, bf16 h/m/l tiles
-  int hpsi_kind;         // single-precision hpsi kernel: 0 bf16 three-term, 1 tf32 three-term, 2 FFT on
-                         // CUDA cores (HFB_HPSI_KERNEL=bf16x3 / tf32x3 at creation, hfb_set_hpsi_kernel)
-  int f64_mma;           // FP64 Gram and rotation on the FP64 tensor cores (HFB_F64_MMA=1) or CUDA cores
+  int hpsi_kind;         // single-precision hpsi kernel: 0 bf16 three-term (default), 1 tf32 three-term, 2 FFT
+                         // on CUDA cores (HFB_HPSI_KERNEL=bf16x3 / tf32x3 / fft at creation, hfb_set_hpsi_kernel)
+  int f64_mma;           // FP64 Gram and rotation on the FP64 tensor cores (default; HFB_F64_MMA=0: CUDA cores)
   long long wait_limit;  // clock cycles any one bounded device wait may take (hfb_set_wait_limit)
   int timeout_probe;     // the next tensor-core hpsi launch runs its timeout path (hfb_arm_timeout_probe)
   // scratch arena: fixed slots, grown on demand (never shrunk)

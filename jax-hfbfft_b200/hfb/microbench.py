@@ -8,7 +8,8 @@ profiler captures).
 Every mode builds the workload's oscillator start and its mean field
 (``static.prepare``), runs the operation ``--warmup`` times and then ``--reps``
 times between CUDA events on the launching stream, and prints one JSON line
-with the mean time per call.  ``--states`` limits hpsi to the first S states
+with the mean time per call; the timed calls run inside an NVTX range
+"timed" (``ncu --nvtx --nvtx-include timed/``).  ``--states`` limits hpsi to the first S states
 (the potentials stay those of the full nucleus), which keeps a profiler
 capture small.
 """
@@ -38,10 +39,12 @@ def _time(fn, warmup, reps):
     s = torch.cuda.current_stream()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")   # lets a profiler select exactly these launches
     e0.record(s)
     for _ in range(reps):
         fn()
     e1.record(s)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / 1e3 / max(reps, 1)
 

@@ -4,7 +4,9 @@ workload (32^3, dx 0.8 fm, 40 + 30 states, SLy4 + volume delta pairing):
 the binding energy's explicit gradient for all eleven Skyrme couplings and
 both pairing strengths, and the proton rms radius's gradient by the
 implicit adjoint (linear-response solve at the fixed point).  Ca48 is
-doubly magic: its BCS gap collapses and the occupations are 0 or 1."""
+doubly magic: its BCS gap all but collapses, the occupations are within
+about 1e-5 of 0 or 1, and the response holds them fixed (the occupation
+response is of the order of their distance from 0 / 1)."""
 import numpy as np
 import pytest
 import torch
@@ -81,7 +83,7 @@ def test_rms_gradient_implicit_adjoint_matches_central_fd(ca48_states):
     from hfb import adjoint
     case, st = ca48_states
     names = ["t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power"]
-    g, info = adjoint.rms_gradient(st, names, tol=1e-10)
+    g, info = adjoint.rms_gradient(st, names, tol=1e-10, allow_fractional=True)
     assert info["residual"] < 1e-10 and info["cg_iterations"] < 500
     fd = adjoint.fd_rms_gradient(case, names, rel_step=1e-4, base=st, tol_r=1e-13)
     th = adjoint.theta_of(st["forces"])
@@ -94,6 +96,6 @@ def test_rms_gradient_implicit_adjoint_matches_central_fd(ca48_states):
 def test_rms_gradient_pairing_strengths_vanish_with_collapsed_pairing(ca48_states):
     from hfb import adjoint
     case, st = ca48_states
-    g, _ = adjoint.rms_gradient(st, ["v0neut", "v0prot"], tol=1e-8)
+    g, _ = adjoint.rms_gradient(st, ["v0neut", "v0prot"], tol=1e-8, allow_fractional=True)
     fd = adjoint.fd_rms_gradient(case, ["v0neut"], rel_step=1e-4, base=st, tol_r=1e-13)
     assert abs(g["v0neut"]) < 1e-9 and abs(g["v0prot"]) < 1e-9 and abs(fd["v0neut"]) < 1e-7
