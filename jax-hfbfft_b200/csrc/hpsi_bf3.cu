@@ -8,9 +8,10 @@
 // current / spin-orbit operator of the axis (meanfield.py:63-141) and the
 // Nyquist term (pi/d)^2 mean_line(B) (-1)^j sum_l (-1)^l psi_l / n.  D on
 // all lines of a state is a real GEMM with K = n: per axis and tile
-//     GEMM 1  e = D psi,           then pointwise o = L_d e (+ local terms),
+//     GEMM 1  e = D psi,           then pointwise o = L_d e,
 //                                  w = L_d psi - B e,
-//     GEMM 2  o + D w,             then the epilogue adds the Nyquist term.
+//     GEMM 2  o + D w,             then the epilogue adds the Nyquist term
+//                                  (and, in the z pass, the local terms).
 //
 // Operands.  Each fp32 value x is split into three bf16 numbers
 // x = h + m + l (h = bf16(x), m = bf16(x - h), l = bf16(x - h - m); both
@@ -384,22 +385,33 @@ __device__ __forceinline__ void hb_tile(const HbArgs& a, const HbThread& t, HbSh
   tc::fence_after();
   const float2 alt = make_float2(sh.alt[t.row][0].x + sh.alt[t.row][1].x, sh.alt[t.row][0].y + sh.alt[t.row][1].y);
 
-  // ---- pointwise: o = L_d e (+ local) over e in the accumulator, w = L_d psi - B e into A
+  // ---- pointwise: o = L_d e over e in the accumulator, w = L_d psi - B e into A.
+  // The global loads of chunk k + 1 are issued before the TMEM accesses of
+  // chunk k (which the compiler cannot reorder memory operations across),
+  // so they are in flight while chunk k is computed.
   const float4* fp = a.F + ((size_t)iq * 3 + AX) * N3 + hb_fidx<N>(L, t.j0);
-  const float4* flp = a.FL + (size_t)iq * N3 + hb_fidx<N>(L, t.j0);
+  float4 fn[4];
+  float2 pn[4];
+  hb_load_chunk<N, AX>(a.psi, cb, 0, pn);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) fn[i] = __ldg(fp + i * kHbLines);
 #pragma unroll
   for (int k = 0; k < G::NCK; ++k) {
+    float4 f[4];
+    float2 pc[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      f[i] = fn[i];
+      pc[i] = pn[i];
+    }
+    if (k + 1 < G::NCK) {
+      hb_load_chunk<N, AX>(a.psi, cb, k + 1, pn);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) fn[i] = __ldg(fp + (4 * (k + 1) + i) * kHbLines);
+    }
     uint32_t er[4], em[4];
     tc::tmem_ld_x4(t.tl + G::DCOL + t.j0 + 4 * k, er);
     tc::tmem_ld_x4(t.tl + G::DCOL + G::N2 + t.j0 + 4 * k, em);
-    float4 f[4], fl[4];
-    float2 pc[4];
-    hb_load_chunk<N, AX>(a.psi, cb, k, pc);   // this thread's psi again (L1 / L2)
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      f[i] = __ldg(fp + (4 * k + i) * kHbLines);
-      if (AX == 2) fl[i] = __ldg(flp + (4 * k + i) * kHbLines);
-    }
     tc::tmem_ld_wait();
     uint32_t orr[4], om[4];
     float2 w[4];
@@ -409,14 +421,7 @@ __device__ __forceinline__ void hb_tile(const HbArgs& a, const HbThread& t, HbSh
       const float2 eo = make_float2(__shfl_xor_sync(0xffffffffu, ev.x, 1), __shfl_xor_sync(0xffffffffu, ev.y, 1));
       const float2 pv = pc[i];
       const float2 po = make_float2(__shfl_xor_sync(0xffffffffu, pv.x, 1), __shfl_xor_sync(0xffffffffu, pv.y, 1));
-      float2 o = hb_l<AX>(f[i], t.kp, ev, eo);
-      if (AX == 2) {
-        // upot psi + sigma.spot psi (meanfield.py:47-58)
-        const float4 gl = fl[i];
-        const float d = gl.x + t.kp * gl.w, s1 = t.kp * gl.z;
-        o.x += d * pv.x + gl.y * po.x + s1 * po.y;
-        o.y += d * pv.y + gl.y * po.y - s1 * po.x;
-      }
+      const float2 o = hb_l<AX>(f[i], t.kp, ev, eo);
       const float2 n = hb_l<AX>(f[i], t.kp, pv, po);
       w[i] = make_float2(n.x - f[i].x * ev.x, n.y - f[i].x * ev.y);
       orr[i] = __float_as_uint(o.x);
@@ -441,46 +446,67 @@ __device__ __forceinline__ void hb_tile(const HbArgs& a, const HbThread& t, HbSh
     }
   }
   __syncthreads();   // the previous pass of the state is complete in memory
-  float2 old[G::PT];
-  if (P > 0 && !sh.bad) {
-    if (AX == 2) {
+
+  // ---- epilogue: o + D w + Nyquist term, 4 points at a time.  The global
+  // inputs of chunk k + 1 are loaded before the TMEM reads of chunk k (as in
+  // the pointwise step), chunk 0's while GEMM 2 runs: the previous pass's
+  // sum (y, x passes), psi and the local fields for the z pass's upot / spin
+  // terms, psi and v_pair for the x pass's outputs.
+  const float nyq = a.nq[AX] * a.bbar[((size_t)iq * 3 + AX) * N * N + L];
+  const float wt = (P == 2 && a.weight) ? (float)a.weight[s] : 1.f;
+  const float wu = (P == 2 && a.weightuv) ? (float)a.weightuv[s] : 0.f;
+  const float* vpq = a.pot + ((size_t)iq * 12 + 2) * N3 + hb_line_base<N, AX>(L) + (size_t)t.j0 * STRIDE;
+  const float4* flp = a.FL + (size_t)iq * N3 + hb_fidx<N>(L, t.j0);
+  double ov_mf = 0.0, ov_po = 0.0;
+  float2 qn[4], on[4];
+  float4 gn[4];
+  float vn[4];
+  auto fetch = [&](int k, float2 (&pc)[4], float2 (&od)[4], float4 (&gl)[4], float (&vp)[4]) {
+    if (P != 1) hb_load_chunk<N, AX>(a.psi, cb, k, pc);
 #pragma unroll
-      for (int i = 0; i < G::PT; ++i) old[i] = make_float2(0.f, 0.f);
-    } else {
-#pragma unroll
-      for (int i = 0; i < G::PT; ++i) old[i] = __ldcg(a.acc + cb + i * STRIDE);
+    for (int i = 0; i < 4; ++i) {
+      if (P > 0) od[i] = __ldcg(a.acc + cb + (4 * k + i) * STRIDE);
+      if (P == 0) gl[i] = __ldg(flp + (4 * k + i) * kHbLines);
+      if (P == 2) vp[i] = __ldg(vpq + (4 * k + i) * STRIDE);
     }
-  }
+  };
+  if (!sh.bad) fetch(0, qn, on, gn, vn);
   if (threadIdx.x == 0 && !tc::mbar_wait(&sh.bar_mma, phase & 1, a.wait_limit)) sh.bad = 1;
   ++phase;
   __syncthreads();
   if (sh.bad) return;
   tc::fence_after();
-
-  // ---- epilogue: o + D w + Nyquist term, 4 points at a time
-  const float nyq = a.nq[AX] * a.bbar[((size_t)iq * 3 + AX) * N * N + L];
-  const float wt = (P == 2 && a.weight) ? (float)a.weight[s] : 1.f;
-  const float wu = (P == 2 && a.weightuv) ? (float)a.weightuv[s] : 0.f;
-  const float* vpq = a.pot + ((size_t)iq * 12 + 2) * N3 + hb_line_base<N, AX>(L) + (size_t)t.j0 * STRIDE;
-  double ov_mf = 0.0, ov_po = 0.0;
 #pragma unroll
   for (int k = 0; k < G::NCK; ++k) {
+    float2 pc[4], old[4];
+    float4 gl[4];
+    float vp[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      pc[i] = qn[i];
+      old[i] = on[i];
+      gl[i] = gn[i];
+      vp[i] = vn[i];
+    }
+    if (k + 1 < G::NCK) fetch(k + 1, qn, on, gn, vn);
     uint32_t dr[4], di[4];
     tc::tmem_ld_x4(t.tl + G::DCOL + t.j0 + 4 * k, dr);
     tc::tmem_ld_x4(t.tl + G::DCOL + G::N2 + t.j0 + 4 * k, di);
-    float vp[4];
-    float2 pc[4];
-    if (P == 2) {
-      hb_load_chunk<N, AX>(a.psi, cb, k, pc);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) vp[i] = __ldg(vpq + (4 * k + i) * STRIDE);
-    }
     tc::tmem_ld_wait();
     float2 z[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const float sg = (i & 1) ? -nyq : nyq;   // (-1)^j, j0 even
       z[i] = make_float2(__uint_as_float(dr[i]) + sg * alt.x, __uint_as_float(di[i]) + sg * alt.y);
+      if (P == 0) {
+        // upot psi + sigma.spot psi (meanfield.py:47-58), with the other
+        // spinor component from the neighbouring lane
+        const float2 pv = pc[i];
+        const float2 po = make_float2(__shfl_xor_sync(0xffffffffu, pv.x, 1), __shfl_xor_sync(0xffffffffu, pv.y, 1));
+        const float d = gl[i].x + t.kp * gl[i].w, s1 = t.kp * gl[i].z;
+        z[i].x += d * pv.x + gl[i].y * po.x + s1 * po.y;
+        z[i].y += d * pv.y + gl[i].y * po.y - s1 * po.x;
+      }
     }
     if (P == 0) {
       float4* d4 = reinterpret_cast<float4*>(a.acc + cb) + 2 * k;
@@ -490,7 +516,7 @@ __device__ __forceinline__ void hb_tile(const HbArgs& a, const HbThread& t, HbSh
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int j = 4 * k + i;
-        a.acc[cb + j * STRIDE] = make_float2(old[j].x + z[i].x, old[j].y + z[i].y);
+        a.acc[cb + j * STRIDE] = make_float2(old[i].x + z[i].x, old[i].y + z[i].y);
       }
     } else {
       // x pass: h psi complete; weights, v_pair psi, overlaps
@@ -498,7 +524,7 @@ __device__ __forceinline__ void hb_tile(const HbArgs& a, const HbThread& t, HbSh
       for (int i = 0; i < 4; ++i) {
         const int j = 4 * k + i;
         const size_t gi = cb + j * STRIDE;
-        const float2 mf = make_float2(old[j].x + z[i].x, old[j].y + z[i].y);
+        const float2 mf = make_float2(old[i].x + z[i].x, old[i].y + z[i].y);
         const float2 pv = pc[i];
         const float2 dl = make_float2(vp[i] * pv.x, vp[i] * pv.y);
         const float2 po = make_float2(wt * mf.x - wu * dl.x, wt * mf.y - wu * dl.y);
