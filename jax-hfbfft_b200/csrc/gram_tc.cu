@@ -135,12 +135,11 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
     const float* pa = psi + (size_t)job.s0[b] * rowf;
     const float* pb = (am == 1 ? hampsi : am == 2 ? hmfpsi : psi) + (size_t)job.s0[b] * rowf;
     const double* vp = job.vp[b];
-    // window w's rows are loaded into registers one window ahead (two
-    // register sets, the loop unrolled by two), so the loads of the next
-    // K block are in flight while this one is split and stored
-    float4 va0[kTcItemsA], vb0[kTcItemsB], va1[kTcItemsA], vb1[kTcItemsB];
-    auto load = [&](int w, float4 (&va)[kTcItemsA], float4 (&vb)[kTcItemsB]) {
+    for (int w = 0; w < nwin; ++w) {
+      const int s = w % kTcStages;
+      if (w >= kTcStages && !wait(&empty[s], (uint32_t)((w / kTcStages - 1) & 1))) break;
       const size_t off = (size_t)(kb0 + w) * 32 + 4 * c;
+      float4 va[kTcItemsA], vb[kTcItemsB];
 #pragma unroll
       for (int i = 0; i < kTcItemsA; ++i)
         if (rowA[i] >= 0) va[i] = __ldg(reinterpret_cast<const float4*>(pa + (size_t)rowA[i] * rowf + off));
@@ -149,11 +148,6 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
         const int j = r0 + kTcRowsPerPass * i;
         if (j < n) vb[i] = __ldg(reinterpret_cast<const float4*>(pb + (size_t)j * rowf + off));
       }
-    };
-    auto store = [&](int w, const float4 (&va)[kTcItemsA], const float4 (&vb)[kTcItemsB]) -> bool {
-      const int s = w % kTcStages;
-      if (w >= kTcStages && !wait(&empty[s], (uint32_t)((w / kTcStages - 1) & 1))) return false;
-      const size_t off = (size_t)(kb0 + w) * 32 + 4 * c;
       float v0 = 1.f, v1 = 1.f;
       if (am == 3) {
         const size_t k = (off / 2) % (size_t)job.n3;
@@ -189,15 +183,6 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
       tc::fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&full[s]);
-      return true;
-    };
-    if (nwin > 0) load(0, va0, vb0);
-    for (int w = 0; w < nwin; w += 2) {
-      if (w + 1 < nwin) load(w + 1, va1, vb1);
-      if (!store(w, va0, vb0)) break;
-      if (w + 1 >= nwin) break;
-      if (w + 2 < nwin) load(w + 2, va0, vb0);
-      if (!store(w + 1, va1, vb1)) break;
     }
   } else if (warp == kTcProducerWarps) {
     // ---------------------------------------------------------------- MMA

@@ -188,7 +188,8 @@ def binding_energy(theta, case, names, tol=1e-10):
 # point rms radius.
 #
 # At the fixed point the occupied states satisfy g_i = q h[rho] psi_i = 0
-# (q = 1 - sum_occ |psi_j><psi_j|; in the converged BCS basis h psi_i =
+# (q = 1 - sum_occ |psi_j><psi_j| over the occupied states of the same
+# isospin as psi_i; in the converged BCS basis h psi_i =
 # e_i psi_i).  A change of theta moves them by dpsi = -H2^-1 dg/dtheta, with
 # H2 the occupied-virtual block of the orbital Hessian,
 #     (H2 v)_i = q (h - e_i) v_i + q dh[v] psi_i,
@@ -268,8 +269,14 @@ class RmsResponse:
              stream_ptr())
 
     def project(self, v):
-        call("hfb_state_project", self.g.ctx.handle, HFB_F64, self.nocc, ptr(self.psi), self.nocc, ptr(v),
-             stream_ptr())
+        """v_j -= sum_i <psi_i|v_j> psi_i within each isospin: orthonormality
+        holds per isospin only, and neutron and proton orbitals of the same
+        shape overlap almost fully, so a projection over all occupied
+        states at once is not a projector."""
+        for lo, hi in ((0, self.nn), (self.nn, self.nocc)):
+            if hi > lo:
+                call("hfb_state_project", self.g.ctx.handle, HFB_F64, hi - lo, ptr(self.psi[lo:hi]), hi - lo,
+                     ptr(v[lo:hi]), stream_ptr())
 
     def hpsi(self, pot, x, out):
         call("hfb_hpsi", self.g.ctx.handle, HFB_F64, ptr(pot), self.nocc, self.nn, ptr(x), ptr(self.ones),

@@ -83,8 +83,8 @@ def test_rms_gradient_implicit_adjoint_matches_central_fd(ca48_states):
     from hfb import adjoint
     case, st = ca48_states
     names = ["t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power"]
-    g, info = adjoint.rms_gradient(st, names, tol=1e-10, allow_fractional=True)
-    assert info["residual"] < 1e-10 and info["cg_iterations"] < 500
+    g, info = adjoint.rms_gradient(st, names, tol=1e-9, allow_fractional=True)
+    assert info["residual"] < 1e-9 and info["cg_iterations"] < 500
     fd = adjoint.fd_rms_gradient(case, names, rel_step=1e-4, base=st, tol_r=1e-13)
     th = adjoint.theta_of(st["forces"])
     for n in names:
