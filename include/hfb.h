@@ -324,6 +324,26 @@ int hfb_state_axpby_diag(hfb_ctx_t ctx, int prec, int nsp, const double* a, cons
                          void* stream);
 int hfb_rms_field(hfb_ctx_t ctx, const double* cm, double r0, double scale, double* field, void* stream);
 
+/* Vector-Jacobian products of hpsi and of the densities (the reference
+ * differentiates meanfield.py:41-159 and densities.py:237-330 with JAX's
+ * reverse mode).  The bilinear form <a|h[P]|b> of hpsi is the integral of
+ * each potential field times the pair density of (a, b) that hfb_add_density
+ * computes (by polarisation), except for the Nyquist term of cderv02
+ * (levels.py:314-330), -(pi/d)^2 mean_line(B) x_N / n on the Nyquist bin of
+ * each line, x_N = sum_j (-1)^j x_j.  These two calls are that term:
+ *   hfb_nyquist_pair:  field[iq][r] += sum_ax (pi/d_ax)^2 / n^2 *
+ *                      sum_{s in iq} w[s] sum_spin Re(conj(a_N) b_N) over
+ *                      the line through r along ax (the bmass cotangent
+ *                      of the term); field device double [2][n^3]
+ *   hfb_nyquist_apply: y_s += scale[s] sum_ax c_ax mean_line(field[iq(s)])
+ *                      (-1)^j x_N, c_ax = -(pi/d_ax)^2 / n (the term with
+ *                      B = field); y must not alias x
+ * States s < nneut are neutrons (iq 0); w and scale are device double[nst]. */
+int hfb_nyquist_pair(hfb_ctx_t ctx, int prec, int nst, int nneut, const void* a, const void* b, const double* w,
+                     double* field, void* stream);
+int hfb_nyquist_apply(hfb_ctx_t ctx, int prec, int nst, int nneut, const double* field, const double* scale,
+                      const void* x, void* y, void* stream);
+
 /* Step-size control and energy history on the device (the host loop of
  * static.py:1864-1878 moved to one device thread, so that iterations can be
  * replayed without host reads in between; no counterpart in the

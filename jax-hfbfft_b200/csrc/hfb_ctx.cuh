@@ -30,7 +30,7 @@ struct hfb_ctx_s {
   long long wait_limit;  // clock cycles any one bounded device wait may take (hfb_set_wait_limit)
   int timeout_probe;     // the next tensor-core hpsi launch runs its timeout path (hfb_arm_timeout_probe)
   // scratch arena: fixed slots, grown on demand (never shrunk)
-  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_HPT, S_LAST, S_NAT, S_RESP, S_RESP2, S_NSLOT };
+  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_HPT, S_LAST, S_NAT, S_RESP, S_RESP2, S_VJP, S_NSLOT };
   void* slot[S_NSLOT];
   size_t slot_bytes[S_NSLOT];
 };

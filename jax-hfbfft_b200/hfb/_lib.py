@@ -106,6 +106,8 @@ _PROTOS = {
     "hfb_state_project": [vp, C.c_int, C.c_int, vp, C.c_int, vp, vp],
     "hfb_state_axpby_diag": [vp, C.c_int, C.c_int, vp, vp, C.c_double, vp, vp],
     "hfb_rms_field": [vp, C.POINTER(C.c_double), C.c_double, C.c_double, vp, vp],
+    "hfb_nyquist_pair": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
+    "hfb_nyquist_apply": [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp],
     "hfb_natural_step": [vp, C.POINTER(NaturalArgs), C.c_int, vp],
     "hfb_natural_symcond": [vp, C.POINTER(NaturalArgs), vp],
     "hfb_natural_end": [vp, C.c_int, C.POINTER(NaturalArgs), vp, vp, vp, vp],
