@@ -101,6 +101,9 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     // FP64 Gram and rotation on the FP64 tensor cores unless HFB_F64_MMA=0
     const char* gk = getenv("HFB_F64_MMA");
     c->f64_mma = (gk && gk[0] == '0') ? 0 : 1;
+    // single-precision Gram K blocks by TMA unless HFB_GRAM_TMA=0
+    const char* gt = getenv("HFB_GRAM_TMA");
+    c->gram_tma = (gt && gt[0] == '0') ? 0 : 1;
     c->wait_limit = kDefaultWaitLimit;
     c->timeout_probe = 0;
   }

@@ -9,7 +9,9 @@
 // and D accumulates hi*hi + hi*lo + lo*hi (the three-term tf32 scheme,
 // about 22 significant bits per product).
 //
-// One CTA owns one 128-row block of A' for one matrix and one slice of K:
+// One CTA owns one 128-row block of A' for one matrix and one slice of K.
+// Two kernels: gram_tma_kernel (the default, below) and gram_tc_kernel,
+// whose producers load through registers:
 //   warps 0-6   load a 32-float K block of the rows from global memory,
 //               split it and store it into a 128-byte-swizzled stage
 //               (3-stage ring);
@@ -24,6 +26,8 @@
 // kernel, which also scatters Re/Im rows into the complex outputs.
 // Every wait is bounded; a timeout latches HFB_ERR_CUDA, drains the MMAs
 // in flight and releases TMEM before returning.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <math.h>
 #include "hfb_ctx.cuh"
 #include "tc_sm100.cuh"
@@ -261,6 +265,262 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same products with the K blocks brought in by the tensor-memory
+// accelerator and A in tensor memory.
+//
+//   warp 0      (one thread) TMA: the raw fp32 K block of the unit's A'
+//               rows (two row ranges: the Psi part and the Psi~ part, each
+//               in 8-row boxes from an 8-row boundary) and of its B rows,
+//               128-byte swizzled, into a 3-stage ring;
+//   warp 1      (one thread) MMAs, A from tensor memory (M = 128, N = np,
+//               K = 8), into one of two accumulators; it owns the TMEM
+//               allocation;
+//   warps 2-7   split B in place (hi over the raw block, lo beside it; rows
+//               past n zeroed, v_pair applied for the fourth matrix);
+//   warps 4-7   also split A' (one row per thread, Psi~ rows formed as
+//               (-im, re)) and store hi and lo into the stage's 64 TMEM
+//               columns;
+//   warps 8-15  drain the accumulators as in gram_tc_kernel.
+// TMEM: accumulators at columns 0 and 160, A stages at 320 + 64 s.  A stage
+// of shared memory is free again when the MMAs that read it commit, which
+// also frees its TMEM A columns.
+constexpr int kGtStages = 3;
+constexpr int kGtThreads = 512;
+constexpr int kGtConvWarps = 6;          // warps 2-7
+constexpr uint32_t kGtRawA = 144 * 128;  // A' raw rows: round8(cnt1) + round8(cnt2) <= 142
+constexpr uint32_t kGtD1 = 160, kGtACol = 320;
+
+__global__ void __launch_bounds__(kGtThreads, 1)
+gram_tma_kernel(TcJob job, const __grid_constant__ CUtensorMap mpsi, const __grid_constant__ CUtensorMap mham,
+                const __grid_constant__ CUtensorMap mhmf, float* __restrict__ part, int* status, long long limit) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ uint64_t raw_full[kGtStages], empty[kGtStages], conv_full[kGtStages], dfull[2], dempty[2], fin;
+  __shared__ uint32_t tbase;
+  __shared__ volatile int abort_flag;
+
+  const int unit = blockIdx.x % job.nunit, chunk = blockIdx.x / job.nunit;
+  const TcUnit U = job.u[unit];
+  const int b = U.b, am = U.a, mb = U.mb;
+  const int n = job.ns[b], np = job.np[b];
+  const int kb0 = (int)((long long)job.kb_total * chunk / job.kchunks);
+  const int kb1 = (int)((long long)job.kb_total * (chunk + 1) / job.kchunks);
+  const int nwin = kb1 - kb0;
+  const uint32_t bbytes = (uint32_t)np * 128, sbytes = kGtRawA + 2 * bbytes;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid & 31;
+  // A' rows g0 .. g0 + 127: Psi rows of states g0 .. (cnt1 of them), then
+  // Psi~ rows of states lo2 - n .. (cnt2 of them)
+  const int g0 = mb * 128;
+  const int cnt1 = max(0, min(n, g0 + 128) - g0);
+  const int lo2 = max(n, g0), cnt2 = max(0, min(2 * n, g0 + 128) - lo2);
+  const int r2 = (cnt1 + 7) / 8 * 8;
+  const int nbox1 = (cnt1 + 7) / 8, nbox2 = (cnt2 + 7) / 8, nboxb = np / 8;
+
+  if (tid == 0) {
+    for (int s = 0; s < kGtStages; ++s) {
+      tc::mbar_init(&raw_full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+      tc::mbar_init(&conv_full[s], kGtConvWarps);
+    }
+    for (int d = 0; d < 2; ++d) {
+      tc::mbar_init(&dfull[d], 1);
+      tc::mbar_init(&dempty[d], kTcEpilogueWarps);
+    }
+    tc::mbar_init(&fin, 1);
+    abort_flag = 0;
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(&tbase, kTcTmemCols);
+    tc::tmem_relinquish();
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tbase;
+
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!tc::mbar_try_wait(bar, parity)) {
+      if (abort_flag) return false;
+      if (clock64() - t0 > limit) {
+        abort_flag = 1;
+        latch_error(status, HFB_ERR_CUDA);
+        return false;
+      }
+    }
+    return true;
+  };
+
+  if (warp == 0) {
+    // ---------------------------------------------------------------- TMA
+    if (lane == 0) {
+      const CUtensorMap* mapb = am == 1 ? &mham : am == 2 ? &mhmf : &mpsi;
+      const uint32_t tx = (uint32_t)(nbox1 + nbox2 + nboxb) * 1024u;
+      const int p0 = job.s0[b] + g0, t0 = job.s0[b] + lo2 - n, q0 = job.s0[b];
+      int issued = 0;
+      for (int w = 0; w < nwin; ++w) {
+        const int s = w % kGtStages;
+        if (w >= kGtStages && !wait(&empty[s], (uint32_t)((w / kGtStages - 1) & 1))) break;
+        unsigned char* st = smem + (size_t)s * sbytes;
+        tc::mbar_arrive_expect_tx(&raw_full[s], tx);
+        const int x = (kb0 + w) * 32;
+        for (int i = 0; i < nbox1; ++i) tc::tma_load_2d(st + i * 1024, &mpsi, x, p0 + 8 * i, &raw_full[s]);
+        for (int i = 0; i < nbox2; ++i)
+          tc::tma_load_2d(st + (r2 / 8 + i) * 1024, &mpsi, x, t0 + 8 * i, &raw_full[s]);
+        for (int i = 0; i < nboxb; ++i)
+          tc::tma_load_2d(st + kGtRawA + i * 1024, mapb, x, q0 + 8 * i, &raw_full[s]);
+        issued = w + 1;
+      }
+      // copies still in flight land before the CTA can exit
+      for (int w = max(0, issued - kGtStages); w < issued; ++w)
+        if (!tc::mbar_wait(&raw_full[w % kGtStages], (uint32_t)((w / kGtStages) & 1), limit))
+          latch_error(status, HFB_ERR_CUDA);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------------------------------------------------------- MMA
+    if (lane == 0) {
+      const uint32_t idesc = tc::idesc_tf32(128, np);
+      for (int w = 0; w < nwin; ++w) {
+        const int s = w % kGtStages, d = w & 1;
+        if (!wait(&conv_full[s], (uint32_t)((w / kGtStages) & 1))) break;
+        if (w >= 2 && !wait(&dempty[d], (uint32_t)((w / 2 - 1) & 1))) break;
+        tc::fence_after();
+        const uint32_t bhi = tc::smem_u32(smem + (size_t)s * sbytes + kGtRawA), blo = bhi + bbytes;
+        const uint32_t dt = tmem + (uint32_t)d * kGtD1, at = tmem + kGtACol + (uint32_t)s * 64;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, k > 0);
+          tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(blo + 32 * k), idesc, 1);
+          tc::mma_tf32_ta(dt, at + 32 + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, 1);
+        }
+        tc::mma_commit(&empty[s]);
+        tc::mma_commit(&dfull[d]);
+      }
+      tc::mma_commit(&fin);
+      if (!tc::mbar_wait(&fin, 0, limit)) latch_error(status, HFB_ERR_CUDA);
+    }
+    __syncwarp();
+  } else if (warp < 8) {
+    // --------------------------------------------------------- converters
+    const int ct = tid - 64;
+    const double* vp = job.vp[b];
+    const int q = warp & 3, r = 32 * q + lane;   // A' row of this thread (warps 4-7)
+    const bool do_a = warp >= 4;
+    int arow = -1;
+    bool tilde = false;
+    if (r < cnt1) {
+      arow = r;
+    } else if (r < cnt1 + cnt2) {
+      arow = r2 + (r - cnt1);
+      tilde = true;
+    }
+    for (int w = 0; w < nwin; ++w) {
+      const int s = w % kGtStages;
+      if (!wait(&raw_full[s], (uint32_t)((w / kGtStages) & 1))) break;
+      unsigned char* st = smem + (size_t)s * sbytes;
+      unsigned char* bh = st + kGtRawA;
+      const size_t xoff = (size_t)(kb0 + w) * 32;
+      for (int e = ct; e < np * 8; e += kGtConvWarps * 32) {
+        const int row = e >> 3, c = e & 7;
+        const uint32_t o = tc::sw128_offset(row, c);
+        float4 v = *reinterpret_cast<const float4*>(bh + o);
+        if (row >= n) {
+          v = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else if (am == 3) {
+          const size_t k = ((xoff + 4 * c) / 2) % (size_t)job.n3;
+          const float v0 = (float)vp[k], v1 = (float)vp[k + 1];
+          v = make_float4(v0 * v.x, v0 * v.y, v1 * v.z, v1 * v.w);
+        }
+        float4 h, l;
+        h.x = tc::to_tf32(v.x); l.x = tc::to_tf32(v.x - h.x);
+        h.y = tc::to_tf32(v.y); l.y = tc::to_tf32(v.y - h.y);
+        h.z = tc::to_tf32(v.z); l.z = tc::to_tf32(v.z - h.z);
+        h.w = tc::to_tf32(v.w); l.w = tc::to_tf32(v.w - h.w);
+        *reinterpret_cast<float4*>(bh + o) = h;
+        *reinterpret_cast<float4*>(bh + bbytes + o) = l;
+      }
+      if (do_a) {
+        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + kGtACol + (uint32_t)s * 64;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+          float hv[16], lv[16];
+#pragma unroll
+          for (int c4 = 0; c4 < 4; ++c4) {
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (arow >= 0) v = *reinterpret_cast<const float4*>(st + tc::sw128_offset(arow, 4 * half + c4));
+            if (tilde) v = make_float4(-v.y, v.x, -v.w, v.z);
+            const float x4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              hv[4 * c4 + i] = tc::to_tf32(x4[i]);
+              lv[4 * c4 + i] = tc::to_tf32(x4[i] - hv[4 * c4 + i]);
+            }
+          }
+          tc::tmem_st16(ta + 16 * half, hv);
+          tc::tmem_st16(ta + 32 + 16 * half, lv);
+        }
+        tc::tmem_st_wait();
+      }
+      tc::fence_proxy_async_smem();
+      tc::fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&conv_full[s]);
+    }
+  } else {
+    // ----------------------------------------------------------- epilogue
+    const int q = warp & 3;
+    const int half = (warp - 8) / 4;
+    const int ng = np / 16, gh = (ng + 1) / 2;
+    const int gbeg = half ? gh : 0, gcnt = half ? ng - gh : gh;
+    float acc[kTcMaxGroups][16];
+#pragma unroll
+    for (int g = 0; g < kTcMaxGroups; ++g)
+#pragma unroll
+      for (int i = 0; i < 16; ++i) acc[g][i] = 0.f;
+    bool ok = true;
+    for (int w = 0; w < nwin; ++w) {
+      const int d = w & 1;
+      if (!wait(&dfull[d], (uint32_t)((w / 2) & 1))) { ok = false; break; }
+      tc::fence_after();
+      const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)d * kGtD1;
+#pragma unroll
+      for (int g = 0; g < kTcMaxGroups; ++g) {
+        if (g < gcnt) {
+          float v[16];
+          tc::tmem_ld16(ta + (uint32_t)((gbeg + g) * 16), v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[g][i] += v[i];
+        }
+      }
+      tc::fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&dempty[d]);
+    }
+    if (ok && !abort_flag) {
+      const int row = q * 32 + lane;
+      float* o = part + ((size_t)blockIdx.x * 128 + row) * kTcMaxNp;
+#pragma unroll
+      for (int g = 0; g < kTcMaxGroups; ++g)
+        if (g < gcnt) {
+#pragma unroll
+          for (int i = 0; i < 16; i += 4)
+            *reinterpret_cast<float4*>(o + (gbeg + g) * 16 + i) =
+                make_float4(acc[g][i], acc[g][i + 1], acc[g][i + 2], acc[g][i + 3]);
+        }
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc::fence_after();
+    tc::tmem_dealloc(tmem, kTcTmemCols);
+  }
+}
+
 struct TcOut {
   double2* p[8];   // [block * 4 + matrix]
 };
@@ -287,6 +547,36 @@ __global__ void gram_tc_reduce_kernel(TcJob job, const float* __restrict__ part,
   double2* out = outs.p[b * 4 + am];
   out[(size_t)i * ldo + j] = make_double2(scale * re, scale * im);
   if (herm && i != j) out[(size_t)j * ldo + i] = make_double2(scale * re, -scale * im);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }();
+  return fn;
+}
+
+// rows x kf fp32 matrix (row pitch kf floats) read in 8-row x 32-float
+// boxes with the 128-byte swizzle; rows past ``rows`` read as zero
+bool encode_state_map(CUtensorMap* m, const void* base, uint64_t kf, int rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || !base || ((uintptr_t)base & 15) || rows <= 0) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)kf, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(kf * sizeof(float))};
+  cuuint32_t box[2] = {32, 8};
+  cuuint32_t es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 }  // namespace
@@ -335,10 +625,28 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
   if (!part) return HFB_ERR_ALLOC;
   int npmax = 16;
   for (int b = 0; b < nblk; ++b) npmax = job.np[b] > npmax ? job.np[b] : npmax;
-  const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)npmax * 128);
-  allow_max_dynamic_smem(gram_tc_kernel);
-  gram_tc_kernel<<<ncta, kTcThreads, smem, st>>>(job, (const float*)psi, (const float*)hampsi,
-                                                 (const float*)hmfpsi, part, c->dev_status);
+  if (c->gram_tma) {
+    // tensor maps over the states as rows of 4 n^3 floats (both spin
+    // components, interleaved re/im), rows up to the last state used
+    int rows = 0;
+    for (int b = 0; b < nblk; ++b)
+      if (ns[b] > 0) rows = s0[b] + ns[b] > rows ? s0[b] + ns[b] : rows;
+    CUtensorMap mp, mh, mm;
+    const uint64_t kf = 4 * (uint64_t)job.n3;
+    if (!encode_state_map(&mp, psi, kf, rows)) return HFB_ERR_CUDA;
+    mh = mp;
+    mm = mp;
+    if (hampsi && !encode_state_map(&mh, hampsi, kf, rows)) return HFB_ERR_CUDA;
+    if (hmfpsi && !encode_state_map(&mm, hmfpsi, kf, rows)) return HFB_ERR_CUDA;
+    const size_t smem = 1024 + (size_t)kGtStages * (kGtRawA + 2 * (size_t)npmax * 128);
+    allow_max_dynamic_smem(gram_tma_kernel);
+    gram_tma_kernel<<<ncta, kGtThreads, smem, st>>>(job, mp, mh, mm, part, c->dev_status, c->wait_limit);
+  } else {
+    const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)npmax * 128);
+    allow_max_dynamic_smem(gram_tc_kernel);
+    gram_tc_kernel<<<ncta, kTcThreads, smem, st>>>(job, (const float*)psi, (const float*)hampsi,
+                                                   (const float*)hmfpsi, part, c->dev_status);
+  }
   HFB_CHECK_LAUNCH();
   TcOut ot;
   for (int q = 0; q < 8; ++q) ot.p[q] = outs_host[q];

@@ -27,6 +27,8 @@ struct hfb_ctx_s {
   int hpsi_kind;         // single-precision hpsi kernel: 0 bf16 three-term (default), 1 tf32 three-term, 2 FFT
                          // on CUDA cores (HFB_HPSI_KERNEL=bf16x3 / tf32x3 / fft at creation, hfb_set_hpsi_kernel)
   int f64_mma;           // FP64 Gram and rotation on the FP64 tensor cores (default; HFB_F64_MMA=0: CUDA cores)
+  int gram_tma;          // single-precision Gram: K blocks by TMA, A in TMEM (default; HFB_GRAM_TMA=0 at creation:
+                         // register-loaded producers)
   long long wait_limit;  // clock cycles any one bounded device wait may take (hfb_set_wait_limit)
   int timeout_probe;     // the next tensor-core hpsi launch runs its timeout path (hfb_arm_timeout_probe)
   // scratch arena: fixed slots, grown on demand (never shrunk)

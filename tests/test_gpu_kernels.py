@@ -377,6 +377,21 @@ def test_gram_tensor_cores_match_cuda_cores(monkeypatch):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n,s0,ns", [(16, 0, 140), (16, 5, 96), (24, 3, 9)])
+def test_gram_tma_matches_register_producers(monkeypatch, n, s0, ns):
+    """The TMA-fed Gram (A in tensor memory, the default) and the
+    register-loaded one (HFB_GRAM_TMA=0 at context creation) compute the
+    same three-term products: equal to within the fp32 accumulation order."""
+    g, a, vp = _gram_case(n, s0, ns, 13)
+    tma = _gram_run(g, a, vp, s0, ns, torch.complex64)
+    monkeypatch.setenv("HFB_GRAM_TMA", "0")
+    g2, _, _ = _gram_case(n, s0, ns, 13)
+    reg = _gram_run(g2, a, vp, s0, ns, torch.complex64)
+    for k in range(4):
+        assert rel(tma[k], reg[k]) < 1e-6, (k, rel(tma[k], reg[k]))
+
+
+@pytest.mark.gpu
 def test_diagstep_single_precision_matches_double():
     """hfb_diagstep on complex64 states (tensor-core Gram, Newton-Schulz
     S^-1/2, register-tiled rotation) against the same step on the complex128
