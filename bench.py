@@ -57,7 +57,7 @@ FALLBACK_HBM_GBS = 6650.0
 # measured by this bench's FP64 leg on a B200 (same algorithm and step-size
 # rule as the oracle).  The reference arm, which cannot afford a converged
 # CPU run of the large workloads, scales its per-iteration time by these.
-FP64_ITERATIONS_TO_1KEV = {"Pb208": 661, "Cr48": 330, "O16": 230}
+FP64_ITERATIONS_TO_1KEV = {"Pb208": 661, "Cr48": 270, "O16": 173}
 # Upper bound on the seconds the reference arm spends on timed iterations.
 REFERENCE_ARM_BUDGET_S = 300.0
 # Both runs continue until the estimated remaining energy change is below
@@ -219,7 +219,7 @@ def fp64_run(case_name, maxiter):
     return dict(E=E, t=t, e_ref=e_ref, converged=converged, iters=len(E), state=st)
 
 
-def mixed_e2e_run(case_name, maxiter, switch_mev=5e-4):
+def mixed_e2e_run(case_name, maxiter, switch_mev=2e-4):
     """Mixed run through hfb.static.statichf_mixed.  The initial states are
     copied from pinned host memory inside the timed region; E_bind, the
     densities and the single-particle energies are read back at the end."""
@@ -421,7 +421,7 @@ def main():
     ap.add_argument("--cpu-full", action="store_true",
                     help="reference arm: run the oracle to convergence (a measured CPU time-to-converge; small "
                          "workloads only)")
-    ap.add_argument("--switch-mev", type=float, default=5e-4,
+    ap.add_argument("--switch-mev", type=float, default=2e-4,
                     help="mixed run: estimated remaining change (MeV) at which FP32 hands over to FP64")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -8,16 +8,18 @@ time, except for the step size x0dmp, which the step-control kernel
 (hfb_step_control) now keeps on the device together with a history of
 E_bind.  A block of iterations -- an even number, because the
 diagonalisation step alternates between the state buffer and its spare --
-is captured once into a CUDA graph and replayed; the host reads the energy
-history once per replay.  Several instances (different nuclei, grids,
-couplings) are captured into the same graph, each on its own stream forked
-from the capture stream, so one graph launch advances all of them.
+is captured once into a CUDA graph per instance and replayed; the host
+reads the energy history once per replay.  Several instances (different
+nuclei, grids, couplings) are advanced by one launch of a composite graph
+whose nodes are copies of the instances' captures (no edges between them,
+so they run as concurrent branches); when instances finish or switch
+precision the composite is rebuilt from the captures at hand, and only the
+instance that switched is captured again.
 
 Requirements of a replay: every scratch buffer of the library has reached
 its size (the warm-up iterations do that, and a slot never shrinks), no
 constraints and no configuration-space sub-iterations, and the precision of
-an instance does not change inside a captured block (the mixed driver
-recaptures when an instance switches to FP64).
+an instance does not change inside a captured block.
 """
 import ctypes as C
 
@@ -44,6 +46,9 @@ class GraphRun:
         self.read = 0              # history entries already read by the host
         self.E = []                # E_bind per iteration (host copy)
         self.prepared = False
+        self.graph = None          # this run's captured block of iterations
+        self.graph_block = None
+        self.graph_dtype = None
 
     def steady_from(self):
         """First iteration index whose device work no longer depends on it."""
@@ -88,6 +93,29 @@ class GraphRun:
             self.read = n
         self.S["grids"].ctx.check(f"graph replay up to iteration {self.i}")
 
+    def capture(self, block):
+        """Capture ``block`` iterations with device step control into this
+        run's own graph (capture only records: the counters restart)."""
+        self.to_device_control()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        i0 = self.i
+        with torch.cuda.graph(g, capture_error_mode="relaxed"):
+            for _ in range(block):
+                self.record()
+        self.i = i0
+        self.count.zero_()
+        self.read = 0
+        torch.cuda.synchronize()
+        self.graph, self.graph_block, self.graph_dtype = g, block, self.st["levels"].psi.dtype
+        return g
+
+    def drop_graph(self):
+        """Back to ordinary iterations: the capture goes, the step size and
+        previous values return to the host."""
+        self.graph = None
+        self.release_device_control()
+
     def release_device_control(self):
         """Back to host control: the step size and previous values from the device."""
         v = self.ctl.cpu().tolist()
@@ -97,46 +125,85 @@ class GraphRun:
         en.sync()
 
 
+def _cuda_ok(res, what):
+    err = res[0] if isinstance(res, tuple) else res
+    if int(err) != 0:
+        raise RuntimeError(f"{what}: CUDA error {int(err)}")
+    return res[1] if isinstance(res, tuple) and len(res) > 1 else None
+
+
+class _Composite:
+    """One executable graph whose nodes are copies of several captured
+    graphs, with no edges between them: one launch runs them all, as
+    concurrent branches."""
+
+    def __init__(self, graphs):
+        from cuda.bindings import runtime as rt
+        self.rt = rt
+        self.graph = _cuda_ok(rt.cudaGraphCreate(0), "cudaGraphCreate")
+        self.exe = None
+        try:
+            for g in graphs:
+                child = rt.cudaGraph_t(init_value=g.raw_cuda_graph())
+                _cuda_ok(rt.cudaGraphAddChildGraphNode(self.graph, None, 0, child), "cudaGraphAddChildGraphNode")
+            self.exe = _cuda_ok(rt.cudaGraphInstantiate(self.graph, 0), "cudaGraphInstantiate")
+        except Exception:
+            self.close()
+            raise
+
+    def launch(self):
+        st = self.rt.cudaStream_t(init_value=torch.cuda.current_stream().cuda_stream)
+        _cuda_ok(self.rt.cudaGraphLaunch(self.exe, st), "cudaGraphLaunch")
+
+    def close(self):
+        if self.exe is not None:
+            self.rt.cudaGraphExecDestroy(self.exe)
+            self.exe = None
+        if self.graph is not None:
+            self.rt.cudaGraphDestroy(self.graph)
+            self.graph = None
+
+
 class BatchGraph:
-    """Captured blocks of iterations of several GraphRuns in one CUDA graph."""
+    """Blocks of iterations of several GraphRuns advanced by one graph
+    launch.  Each run's block is captured once into its own graph (again
+    only when its precision changes), and the batch is the composite of
+    those graphs: when instances finish or switch, the batch is recomposed
+    from the captures it already has instead of recapturing every
+    instance."""
 
     def __init__(self, runs, block=10):
         if block % 2:
             raise ValueError("block must be even (the diagonalisation step alternates two state buffers)")
         self.runs = list(runs)
         self.block = block
-        self.graph = None
-        self.base = [r.i for r in self.runs]
+        self.comp = None
+        self.streams = None
 
     def capture(self):
         for r in self.runs:
-            r.to_device_control()
-        torch.cuda.synchronize()
-        g = torch.cuda.CUDAGraph()
-        streams = [torch.cuda.Stream() for _ in self.runs]
-        starts = [r.i for r in self.runs]
-        with torch.cuda.graph(g, capture_error_mode="relaxed"):
-            cur = torch.cuda.current_stream()
-            for r, s in zip(self.runs, streams):
-                s.wait_stream(cur)
-                with torch.cuda.stream(s):
-                    for _ in range(self.block):
-                        r.record()
-            for s in streams:
-                cur.wait_stream(s)
-        # capture only recorded the work: the iteration counters restart
-        for r, i0 in zip(self.runs, starts):
-            r.i = i0
-            r.count.zero_()
-            r.read = 0
-        self.graph = g
-        self.streams = streams
-        torch.cuda.synchronize()
+            if r.graph is None or r.graph_block != self.block or r.graph_dtype != r.st["levels"].psi.dtype:
+                r.capture(self.block)
+        try:
+            self.comp = _Composite([r.graph for r in self.runs])
+        except (ImportError, RuntimeError):
+            # without the composite: each run's graph on a stream of its own
+            self.comp = None
+            self.streams = [torch.cuda.Stream() for _ in self.runs]
         return self
 
     def replay(self):
         """Advance every instance by one block of iterations."""
-        self.graph.replay()
+        if self.comp is not None:
+            self.comp.launch()
+        else:
+            cur = torch.cuda.current_stream()
+            for r, s in zip(self.runs, self.streams):
+                s.wait_stream(cur)
+                with torch.cuda.stream(s):
+                    r.graph.replay()
+            for s in self.streams:
+                cur.wait_stream(s)
         for r in self.runs:
             r.i += self.block
         torch.cuda.synchronize()
@@ -144,28 +211,36 @@ class BatchGraph:
             r.collect()
 
     def release(self):
-        for r in self.runs:
-            r.release_device_control()
-        self.graph = None
+        """Drop the composite; the runs keep their captures and device control."""
+        if self.comp is not None:
+            self.comp.close()
+            self.comp = None
 
 
-def solve(states, switch_mev=5e-4, stop_mev=5e-5, floor_mev=5e-5, maxiter=4000, block=10, graph_min=60,
-          on_block=None, tune=True):
+def solve(states, switch_mev=2e-4, stop_mev=5e-5, floor_mev=5e-5, maxiter=4000, block=10, graph_min=60,
+          on_block=None, tune=True, fp32_min_points=static.FP32_MIN_POINTS):
     """Mixed-precision solves of several instances (states with complex64
     psi from hfb.config.setup) advanced together: ordinary iterations
     through the start-up phases, then graph replays of ``block`` iterations
     of every active instance per launch.  Each instance follows the
     precision rule of hfb.static.statichf_mixed (FP32 until the estimated
     remaining change is below ``switch_mev`` or the FP32 noise floor is
-    reached, then FP64 until it is below ``stop_mev``); the graph is
-    recaptured whenever an instance switches or finishes.  With ``tune``
+    reached, then FP64 until it is below ``stop_mev``); an instance's block
+    is captured again only when it switches precision, and the batch graph
+    is recomposed from the captures whenever an instance switches or
+    finishes.  Problems smaller than ``fp32_min_points`` (states times grid
+    points) run in FP64 throughout.  With ``tune``
     the single-precision hpsi kernel of each instance is chosen by
     measurement (hfb.tune, cached per grid and state count).  Returns one
     dict per instance: energies, the precision switch iteration, iterations
     and the hpsi kernel used."""
     from . import tune as _tune
+    for s in states:
+        if s["levels"].psi.dtype != torch.complex128 and s["levels"].nstmax * s["grids"].n3 < fp32_min_points:
+            static.to_precision(s, torch.complex128)
     runs = [GraphRun(s) for s in states]
-    info = [dict(switch=None, done=False, prec="f32", hpsi=None) for _ in runs]
+    info = [dict(switch=None if s["levels"].psi.dtype != torch.complex128 else 0, done=False,
+                 prec="f32" if s["levels"].psi.dtype != torch.complex128 else "f64", hpsi=None) for s in states]
     for r, inf in zip(runs, info):
         r.start()
         if tune:
@@ -196,8 +271,10 @@ def solve(states, switch_mev=5e-4, stop_mev=5e-5, floor_mev=5e-5, maxiter=4000, 
         for k in list(active):
             r, inf = runs[k], info[k]
             if inf["done"]:
+                r.drop_graph()
                 active.remove(k)
             elif inf["prec"] == "f64" and r.st["levels"].psi.dtype != torch.complex128:
+                r.drop_graph()
                 static.to_precision(r.st, torch.complex128)
                 tail_start[k] = len(r.E) - 1
                 # the FP64 arrays are new: ordinary iterations grow the

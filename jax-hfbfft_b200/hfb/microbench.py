@@ -4,6 +4,7 @@ profiler captures).
     python -m hfb.microbench hpsi    [--case Pb208] [--states S] [--prec f32|f64] [--reps R]
     python -m hfb.microbench gram    [--case Pb208] [--prec f32|f64] [--reps R]
     python -m hfb.microbench iterate [--case Pb208] [--prec f32|f64] [--reps R] [--skip N]
+    python -m hfb.microbench kernels [--case Pb208] [--prec f32|f64] [--reps R] [--skip N] [--top K]
 
 Every mode builds the workload's oscillator start and its mean field
 (``static.prepare``), runs the operation ``--warmup`` times and then ``--reps``
@@ -111,18 +112,49 @@ def run_iterate(args, dtype):
                 launches_setup=l0, launches_per_iteration=(l2 - l1) / (args.warmup + args.reps))
 
 
+def run_kernels(args, dtype):
+    """Per-kernel device time of ``--reps`` iterations after the untimed
+    ones, from the CUDA activity trace of torch.profiler (kernels overlap
+    as in an ordinary run; the trace adds host-side overhead only)."""
+    from torch.profiler import profile, ProfilerActivity
+    st, S = _setup(args.case, dtype)
+    i = 0
+    for _ in range(args.skip + args.warmup):
+        i += 1
+        static.iterate(i, **S)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(args.reps):
+            i += 1
+            static.iterate(i, **S)
+        torch.cuda.synchronize()
+    rows = []
+    for e in prof.key_averages():
+        t = getattr(e, "device_time_total", None)
+        if t is None:
+            t = getattr(e, "cuda_time_total", 0.0)
+        if t > 0:
+            rows.append((t, e.count, e.key))
+    rows.sort(reverse=True)
+    tot = sum(r[0] for r in rows)
+    top = [dict(kernel=k[:90], calls_per_iteration=c / args.reps, us_per_iteration=t / args.reps,
+                share=t / tot) for t, c, k in rows[:args.top]]
+    return dict(op="kernels", us_per_iteration_total=tot / args.reps, kernels=top)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m hfb.microbench")
-    ap.add_argument("op", choices=("hpsi", "gram", "iterate"))
+    ap.add_argument("op", choices=("hpsi", "gram", "iterate", "kernels"))
     ap.add_argument("--case", default="Pb208")
     ap.add_argument("--prec", default="f32", choices=("f32", "f64"))
     ap.add_argument("--states", type=int, default=0)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--skip", type=int, default=0, help="iterate: untimed iterations before the warm-up")
+    ap.add_argument("--top", type=int, default=25, help="kernels: rows to print")
     args = ap.parse_args(argv)
     dtype = torch.complex64 if args.prec == "f32" else torch.complex128
-    fn = {"hpsi": run_hpsi, "gram": run_gram, "iterate": run_iterate}[args.op]
+    fn = {"hpsi": run_hpsi, "gram": run_gram, "iterate": run_iterate, "kernels": run_kernels}[args.op]
     res = fn(args, dtype)
     res.update(case=args.case, prec=args.prec, reps=args.reps)
     print(json.dumps(res), flush=True)

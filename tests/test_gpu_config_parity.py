@@ -69,8 +69,8 @@ def test_mixed_driver_matches_reference_o16():
     from hfb import static
     ref = _fixture("o16_n24")
     st = _setup("o16_n24", torch.complex64)
-    hist, sw = static.statichf_mixed(st, maxiter=3000, stop_mev=1e-7)
-    assert sw is not None and hist[-1][2] == "f64"
+    hist, sw = static.statichf_mixed(st, maxiter=3000, stop_mev=1e-7, fp32_min_points=0)
+    assert sw is not None and sw > 0 and hist[0][2] == "f32" and hist[-1][2] == "f64"
     assert abs(st["energies"].ehf - float(ref["ehf"])) <= 1e-3
     _, rms, _ = hfb.output.rms_radii(st["densities"], st["grids"])
     assert np.max(np.abs(np.array(rms) - ref["rms"])) <= 1e-4

@@ -59,7 +59,8 @@ def test_gram_f64_against_numpy(kind, n, ns):
             # diagonal keeps the rounding-level imaginary part of its sum
             off = ~np.eye(ns, dtype=bool)
             assert np.array_equal(o[a][off], np.conj(o[a].T)[off])
-            assert np.max(np.abs(np.diag(o[a]).imag)) <= 1e-13 * np.max(np.abs(o[a]))
+            if a != 2:            # random hmfpsi: its diagonal is not real
+                assert np.max(np.abs(np.diag(o[a]).imag)) <= 1e-13 * np.max(np.abs(o[a]))
         assert e < 1e-12, (a, e)
 
 

@@ -67,15 +67,26 @@ def test_two_instances_in_one_graph_match_their_solo_runs():
     bg.release()
     for r, ref in zip(runs, refs):
         assert np.max(np.abs(np.array(r.E) - ref)) < 1e-9
+    # the second instance leaves; the batch is recomposed from the first
+    # one's existing capture, which carries on where it stopped
+    g0 = runs[0].graph
+    runs[1].drop_graph()
+    bg = graph.BatchGraph(runs[:1], block=10).capture()
+    assert runs[0].graph is g0
+    bg.replay()
+    bg.release()
+    ref = _plain(cases[0], 42, torch.complex128)
+    assert np.max(np.abs(np.array(runs[0].E) - ref)) < 1e-9
 
 
 def test_graph_solve_mixed_precision_converges_like_the_host_driver():
     from hfb import config, graph, static
     case = _case(24)
     st = config.setup(copy.deepcopy(case), dtype=torch.complex64)
-    hist, _ = static.statichf_mixed(st, maxiter=3000, stop_mev=5e-6)
-    res = graph.solve([config.setup(copy.deepcopy(case), dtype=torch.complex64)], stop_mev=5e-6, maxiter=3000)
-    assert res[0]["switch"] is not None
+    hist, _ = static.statichf_mixed(st, maxiter=3000, stop_mev=5e-6, fp32_min_points=0)
+    res = graph.solve([config.setup(copy.deepcopy(case), dtype=torch.complex64)], stop_mev=5e-6, maxiter=3000,
+                      fp32_min_points=0)
+    assert res[0]["switch"] is not None and res[0]["switch"] > 0
     assert abs(res[0]["E"][-1] - hist[-1][1]) < 1e-3
 
 
