@@ -5,6 +5,7 @@
 #include <string.h>
 #include <atomic>
 #include <vector>
+#include <cudaTypedefs.h>
 #include "hfb_ctx.cuh"
 
 namespace hfb {
@@ -13,6 +14,34 @@ static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 static thread_local int t_last_cuda_error = 0;
 void note_cuda_error(int e) { t_last_cuda_error = e; }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }();
+  return fn;
+}
+
+bool encode_fp32_rows_map(CUtensorMap* m, const void* base, uint64_t row_floats, uint64_t rows, uint32_t box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || !base || ((uintptr_t)base & 15) || rows == 0 || box_rows == 0 || box_rows > 256) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)row_floats, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(row_floats * sizeof(float))};
+  cuuint32_t box[2] = {32, box_rows};
+  cuuint32_t es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 int coulomb_init(hfb_ctx_s* c);  // skyrme.cu
 int hpsi_tc_prepare(hfb_ctx_s* c);   // hpsi_tc.cu
@@ -101,9 +130,9 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     // FP64 Gram and rotation on the FP64 tensor cores unless HFB_F64_MMA=0
     const char* gk = getenv("HFB_F64_MMA");
     c->f64_mma = (gk && gk[0] == '0') ? 0 : 1;
-    // single-precision Gram K blocks by TMA unless HFB_GRAM_TMA=0
-    const char* gt = getenv("HFB_GRAM_TMA");
-    c->gram_tma = (gt && gt[0] == '0') ? 0 : 1;
+    // single-precision Gram and rotation fed by TMA unless HFB_TMA_FEED=0
+    const char* gt = getenv("HFB_TMA_FEED");
+    c->tma_feed = (gt && gt[0] == '0') ? 0 : 1;
     c->wait_limit = kDefaultWaitLimit;
     c->timeout_probe = 0;
   }

@@ -26,8 +26,6 @@
 // kernel, which also scatters Re/Im rows into the complex outputs.
 // Every wait is bounded; a timeout latches HFB_ERR_CUDA, drains the MMAs
 // in flight and releases TMEM before returning.
-#include <cuda.h>
-#include <cudaTypedefs.h>
 #include <math.h>
 #include "hfb_ctx.cuh"
 #include "tc_sm100.cuh"
@@ -549,36 +547,6 @@ __global__ void gram_tc_reduce_kernel(TcJob job, const float* __restrict__ part,
   if (herm && i != j) out[(size_t)j * ldo + i] = make_double2(scale * re, -scale * im);
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no
-// link against the driver library).
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess) {
-      cudaGetLastError();
-      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
-    }
-    return (PFN_cuTensorMapEncodeTiled_v12000)p;
-  }();
-  return fn;
-}
-
-// rows x kf fp32 matrix (row pitch kf floats) read in 8-row x 32-float
-// boxes with the 128-byte swizzle; rows past ``rows`` read as zero
-bool encode_state_map(CUtensorMap* m, const void* base, uint64_t kf, int rows) {
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc || !base || ((uintptr_t)base & 15) || rows <= 0) return false;
-  cuuint64_t dims[2] = {(cuuint64_t)kf, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)(kf * sizeof(float))};
-  cuuint32_t box[2] = {32, 8};
-  cuuint32_t es[2] = {1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, es,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
 }  // namespace
 
 // Returns HFB_ERR_UNSUPPORTED_GRID when a block exceeds kTcMaxNp states
@@ -625,7 +593,7 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
   if (!part) return HFB_ERR_ALLOC;
   int npmax = 16;
   for (int b = 0; b < nblk; ++b) npmax = job.np[b] > npmax ? job.np[b] : npmax;
-  if (c->gram_tma) {
+  if (c->tma_feed) {
     // tensor maps over the states as rows of 4 n^3 floats (both spin
     // components, interleaved re/im), rows up to the last state used
     int rows = 0;
@@ -633,11 +601,11 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
       if (ns[b] > 0) rows = s0[b] + ns[b] > rows ? s0[b] + ns[b] : rows;
     CUtensorMap mp, mh, mm;
     const uint64_t kf = 4 * (uint64_t)job.n3;
-    if (!encode_state_map(&mp, psi, kf, rows)) return HFB_ERR_CUDA;
+    if (!encode_fp32_rows_map(&mp, psi, kf, rows, 8)) return HFB_ERR_CUDA;
     mh = mp;
     mm = mp;
-    if (hampsi && !encode_state_map(&mh, hampsi, kf, rows)) return HFB_ERR_CUDA;
-    if (hmfpsi && !encode_state_map(&mm, hmfpsi, kf, rows)) return HFB_ERR_CUDA;
+    if (hampsi && !encode_fp32_rows_map(&mh, hampsi, kf, rows, 8)) return HFB_ERR_CUDA;
+    if (hmfpsi && !encode_fp32_rows_map(&mm, hmfpsi, kf, rows, 8)) return HFB_ERR_CUDA;
     const size_t smem = 1024 + (size_t)kGtStages * (kGtRawA + 2 * (size_t)npmax * 128);
     allow_max_dynamic_smem(gram_tma_kernel);
     gram_tma_kernel<<<ncta, kGtThreads, smem, st>>>(job, mp, mh, mm, part, c->dev_status, c->wait_limit);

@@ -1,5 +1,6 @@
 // Library context: grid, device constants and the scratch arena.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "../../include/hfb.h"
 #include "hfb_common.cuh"
@@ -27,8 +28,8 @@ struct hfb_ctx_s {
   int hpsi_kind;         // single-precision hpsi kernel: 0 bf16 three-term (default), 1 tf32 three-term, 2 FFT
                          // on CUDA cores (HFB_HPSI_KERNEL=bf16x3 / tf32x3 / fft at creation, hfb_set_hpsi_kernel)
   int f64_mma;           // FP64 Gram and rotation on the FP64 tensor cores (default; HFB_F64_MMA=0: CUDA cores)
-  int gram_tma;          // single-precision Gram: K blocks by TMA, A in TMEM (default; HFB_GRAM_TMA=0 at creation:
-                         // register-loaded producers)
+  int tma_feed;          // single-precision Gram and rotation: K blocks by TMA, A in TMEM (default;
+                         // HFB_TMA_FEED=0 at creation: producers that load through registers)
   long long wait_limit;  // clock cycles any one bounded device wait may take (hfb_set_wait_limit)
   int timeout_probe;     // the next tensor-core hpsi launch runs its timeout path (hfb_arm_timeout_probe)
   // scratch arena: fixed slots, grown on demand (never shrunk)
@@ -72,6 +73,11 @@ inline void allow_max_dynamic_smem(F* fn) {
     cudaGetLastError();
 }
 void note_cuda_error(int e);   // the CUDA error behind the last HFB_ERR_CUDA of this host thread
+// Tensor map of a rows x row_floats fp32 matrix (row pitch row_floats) read in
+// box_rows x 32-float boxes with the 128-byte swizzle, rows past ``rows``
+// reading as zero; false when the driver's encoder is unavailable or the
+// base is not 16-byte aligned.
+bool encode_fp32_rows_map(CUtensorMap* m, const void* base, uint64_t row_floats, uint64_t rows, uint32_t box_rows);
 void count_launch();
 
 #define HFB_CHECK_LAUNCH()                                            \

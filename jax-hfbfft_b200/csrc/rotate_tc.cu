@@ -20,6 +20,9 @@
 // write the finished outputs (consecutive lanes hold consecutive grid
 // points, so the stores are coalesced).  Every wait is bounded; a timeout
 // latches HFB_ERR_CUDA, drains the MMAs in flight and releases TMEM.
+// rotate_tma_kernel (the default; HFB_TMA_FEED=0 at context creation selects
+// rotate_tc_kernel) brings the psiT blocks in by TMA and splits A into
+// tensor memory.
 #include <math.h>
 #include "hfb_ctx.cuh"
 #include "tc_sm100.cuh"
@@ -277,6 +280,200 @@ rotate_tc_kernel(RtJob job, const float* __restrict__ psiT, const unsigned char*
   }
 }
 
+// The same rotation with the psiT K blocks brought in by the tensor-memory
+// accelerator (one 128-row x 32-float swizzled box per K block, beside the
+// bulk copy of the B tiles) and A split into tensor memory:
+//   warp 0      (one thread) TMA + bulk copy into a 3-stage ring;
+//   warp 1      (one thread) MMAs with A from TMEM; owns the TMEM allocation;
+//   warps 4-7   split A (one row per thread) into the stage's 64 TMEM columns;
+//   warps 8-15  drain and store as in rotate_tc_kernel.
+// TMEM: accumulators at columns 0 and 160, A stages at 320 + 64 s.
+constexpr uint32_t kRqRawA = 128 * 128;
+constexpr uint32_t kRqStage = kRqRawA + 2 * kRtBBytes;
+constexpr int kRqConvWarps = 4;
+constexpr uint32_t kRqD1 = 160, kRqACol = 320;
+
+__global__ void __launch_bounds__(kRtThreads, 1)
+rotate_tma_kernel(RtJob job, const __grid_constant__ CUtensorMap mpt, const unsigned char* __restrict__ bt,
+                  float2* __restrict__ out1, float2* __restrict__ out2, int* status, long long limit) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ uint64_t raw_full[kRtStages], empty[kRtStages], conv_full[kRtStages], dfull[2], dempty[2], fin;
+  __shared__ uint32_t tbase;
+  __shared__ volatile int abort_flag;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid & 31;
+  const int my_tasks = job.ntask > (int)blockIdx.x ? (job.ntask - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int nwin = my_tasks * job.nkb;
+
+  if (tid == 0) {
+    for (int s = 0; s < kRtStages; ++s) {
+      tc::mbar_init(&raw_full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+      tc::mbar_init(&conv_full[s], kRqConvWarps);
+    }
+    for (int d = 0; d < 2; ++d) {
+      tc::mbar_init(&dfull[d], 1);
+      tc::mbar_init(&dempty[d], kRtEpilogueWarps);
+    }
+    tc::mbar_init(&fin, 1);
+    abort_flag = 0;
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(&tbase, kRtTmemCols);
+    tc::tmem_relinquish();
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tbase;
+
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!tc::mbar_try_wait(bar, parity)) {
+      if (abort_flag) return false;
+      if (clock64() - t0 > limit) {
+        abort_flag = 1;
+        latch_error(status, HFB_ERR_CUDA);
+        return false;
+      }
+    }
+    return true;
+  };
+  auto task_of = [&](int w) { return (int)blockIdx.x + (w / job.nkb) * (int)gridDim.x; };
+
+  if (warp == 0) {
+    // ------------------------------------------------------- TMA and bulk
+    if (lane == 0) {
+      int issued = 0;
+      for (int w = 0; w < nwin; ++w) {
+        const int s = w % kRtStages;
+        if (w >= kRtStages && !wait(&empty[s], (uint32_t)((w / kRtStages - 1) & 1))) break;
+        const int t = task_of(w), kb = w % job.nkb;
+        const int tile = t / job.nchunk, ch = t % job.nchunk;
+        unsigned char* st = smem + (size_t)s * kRqStage;
+        tc::mbar_arrive_expect_tx(&raw_full[s], kRqRawA + 2 * kRtBBytes);
+        tc::tma_load_2d(st, &mpt, kb * 32, tile * 128, &raw_full[s]);
+        tc::bulk_g2s(st + kRqRawA, bt + ((size_t)ch * job.nkb + kb) * 2 * kRtBBytes, 2 * kRtBBytes, &raw_full[s]);
+        issued = w + 1;
+      }
+      for (int w = max(0, issued - kRtStages); w < issued; ++w)
+        if (!tc::mbar_wait(&raw_full[w % kRtStages], (uint32_t)((w / kRtStages) & 1), limit))
+          latch_error(status, HFB_ERR_CUDA);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------------------------------------------------------- MMA
+    if (lane == 0) {
+      const uint32_t idesc = tc::idesc_tf32(128, kRtN);
+      for (int w = 0; w < nwin; ++w) {
+        const int s = w % kRtStages, d = w & 1;
+        if (!wait(&conv_full[s], (uint32_t)((w / kRtStages) & 1))) break;
+        if (w >= 2 && !wait(&dempty[d], (uint32_t)((w / 2 - 1) & 1))) break;
+        tc::fence_after();
+        const uint32_t bhi = tc::smem_u32(smem + (size_t)s * kRqStage + kRqRawA), blo = bhi + kRtBBytes;
+        const uint32_t dt = tmem + (uint32_t)d * kRqD1, at = tmem + kRqACol + (uint32_t)s * 64;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, k > 0);
+          tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(blo + 32 * k), idesc, 1);
+          tc::mma_tf32_ta(dt, at + 32 + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, 1);
+        }
+        tc::mma_commit(&empty[s]);
+        tc::mma_commit(&dfull[d]);
+      }
+      tc::mma_commit(&fin);
+      if (!tc::mbar_wait(&fin, 0, limit)) latch_error(status, HFB_ERR_CUDA);
+    }
+    __syncwarp();
+  } else if (warp >= 4 && warp < 8) {
+    // ------------------------------------------------------- A converters
+    const int q = warp & 3, r = 32 * q + lane;
+    for (int w = 0; w < nwin; ++w) {
+      const int s = w % kRtStages;
+      if (!wait(&raw_full[s], (uint32_t)((w / kRtStages) & 1))) break;
+      const unsigned char* st = smem + (size_t)s * kRqStage;
+      const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + kRqACol + (uint32_t)s * 64;
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        float hv[16], lv[16];
+#pragma unroll
+        for (int c4 = 0; c4 < 4; ++c4) {
+          const float4 v = *reinterpret_cast<const float4*>(st + tc::sw128_offset(r, 4 * half + c4));
+          const float x4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            hv[4 * c4 + i] = tc::to_tf32(x4[i]);
+            lv[4 * c4 + i] = tc::to_tf32(x4[i] - hv[4 * c4 + i]);
+          }
+        }
+        tc::tmem_st16(ta + 16 * half, hv);
+        tc::tmem_st16(ta + 32 + 16 * half, lv);
+      }
+      tc::tmem_st_wait();
+      tc::fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&conv_full[s]);
+    }
+  } else if (warp >= 8) {
+    // ----------------------------------------------------------- epilogue
+    const int q = warp & 3;
+    const int half = (warp - 8) / 4;
+    const int gbeg = half ? kRtMaxGroups : 0, gcnt = half ? kRtGroups - kRtMaxGroups : kRtMaxGroups;
+    float acc[kRtMaxGroups][16];
+#pragma unroll
+    for (int g = 0; g < kRtMaxGroups; ++g)
+#pragma unroll
+      for (int i = 0; i < 16; ++i) acc[g][i] = 0.f;
+    for (int w = 0; w < nwin; ++w) {
+      const int d = w & 1;
+      if (!wait(&dfull[d], (uint32_t)((w / 2) & 1))) break;
+      tc::fence_after();
+      const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)d * kRqD1;
+#pragma unroll
+      for (int g = 0; g < kRtMaxGroups; ++g) {
+        if (g < gcnt) {
+          float v[16];
+          tc::tmem_ld16(ta + (uint32_t)((gbeg + g) * 16), v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[g][i] += v[i];
+        }
+      }
+      tc::fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&dempty[d]);
+      if (w % job.nkb == job.nkb - 1) {
+        const int t = task_of(w);
+        const int tile = t / job.nchunk, ch = t % job.nchunk;
+        const size_t k = (size_t)tile * 128 + q * 32 + lane;
+#pragma unroll
+        for (int g = 0; g < kRtMaxGroups; ++g) {
+          if (g < gcnt) {
+#pragma unroll
+            for (int i = 0; i < 16; i += 2) {
+              const int j = (ch * kRtN + (gbeg + g) * 16 + i) / 2;
+              if (k < job.K && !abort_flag) {
+                const float2 v = make_float2(acc[g][i], acc[g][i + 1]);
+                if (j < job.ns) out1[(size_t)j * job.K + k] = v;
+                else if (j < 2 * job.ns) out2[(size_t)(j - job.ns) * job.K + k] = v;
+              }
+              acc[g][i] = 0.f;
+              acc[g][i + 1] = 0.f;
+            }
+          }
+        }
+      }
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc::fence_after();
+    tc::tmem_dealloc(tmem, kRtTmemCols);
+  }
+}
+
 }  // namespace
 
 // out1 = psi U, out2 = psi L for ns complex64 states at psi (offset already
@@ -314,10 +511,18 @@ int rotate_tc_launch(hfb_ctx_s* c, int ns, const void* psi, const double2* U, co
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   }
   const int grid = job.ntask < nsm ? job.ntask : nsm;
-  const size_t smem = 1024 + (size_t)kRtStages * kRtStage;
-  allow_max_dynamic_smem(rotate_tc_kernel);
-  rotate_tc_kernel<<<grid, kRtThreads, smem, st>>>(job, (const float*)psiT, bt, (float2*)out1, (float2*)out2,
-                                                   c->dev_status);
+  CUtensorMap mpt;
+  if (c->tma_feed && encode_fp32_rows_map(&mpt, psiT, 2 * (uint64_t)job.ldT, K, 128)) {
+    const size_t smem = 1024 + (size_t)kRtStages * kRqStage;
+    allow_max_dynamic_smem(rotate_tma_kernel);
+    rotate_tma_kernel<<<grid, kRtThreads, smem, st>>>(job, mpt, bt, (float2*)out1, (float2*)out2, c->dev_status,
+                                                      c->wait_limit);
+  } else {
+    const size_t smem = 1024 + (size_t)kRtStages * kRtStage;
+    allow_max_dynamic_smem(rotate_tc_kernel);
+    rotate_tc_kernel<<<grid, kRtThreads, smem, st>>>(job, (const float*)psiT, bt, (float2*)out1, (float2*)out2,
+                                                     c->dev_status);
+  }
   HFB_CHECK_LAUNCH();
   return HFB_OK;
 }

@@ -380,11 +380,11 @@ def test_gram_tensor_cores_match_cuda_cores(monkeypatch):
 @pytest.mark.parametrize("n,s0,ns", [(16, 0, 140), (16, 5, 96), (24, 3, 9)])
 def test_gram_tma_matches_register_producers(monkeypatch, n, s0, ns):
     """The TMA-fed Gram (A in tensor memory, the default) and the
-    register-loaded one (HFB_GRAM_TMA=0 at context creation) compute the
+    register-loaded one (HFB_TMA_FEED=0 at context creation) compute the
     same three-term products: equal to within the fp32 accumulation order."""
     g, a, vp = _gram_case(n, s0, ns, 13)
     tma = _gram_run(g, a, vp, s0, ns, torch.complex64)
-    monkeypatch.setenv("HFB_GRAM_TMA", "0")
+    monkeypatch.setenv("HFB_TMA_FEED", "0")
     g2, _, _ = _gram_case(n, s0, ns, 13)
     reg = _gram_run(g2, a, vp, s0, ns, torch.complex64)
     for k in range(4):
@@ -430,6 +430,35 @@ def test_diagstep_single_precision_matches_double():
     e32 = l32.sp_energy.cpu().numpy()
     e64 = l64.sp_energy.cpu().numpy()
     assert np.max(np.abs(np.sort(e32) - np.sort(e64))) < 2e-2
+
+
+@pytest.mark.gpu
+def test_diagstep_tma_feed_matches_register_producers(monkeypatch):
+    """One single-precision diagstep on Pb208 states (three 128-row Gram
+    blocks for the neutrons, rotation tasks over 48^3 x 2 grid points) with
+    the TMA-fed Gram and rotation (the default) and with the register-loaded
+    producers (HFB_TMA_FEED=0 at context creation): the same three-term
+    products, so the rotated states and the single-particle energies agree
+    to single-precision rounding."""
+    from hfb import config, static
+
+    def run():
+        st = config.setup(config.case_dict("Pb208"), dtype=torch.complex128)
+        S = {k: st[k] for k in static._STATE_KEYS}
+        static.prepare(**S)
+        for i in (1, 2):
+            static.iterate(i, **S)
+        static.to_precision(st, torch.complex64)
+        static.diagstep(st["energies"], st["forces"], st["grids"], st["levels"], st["static"], True, True)
+        torch.cuda.synchronize()
+        st["grids"].ctx.check("diagstep")
+        return st["levels"].psi.detach().clone(), st["levels"].sp_energy.detach().cpu().numpy().copy()
+
+    p1, e1 = run()
+    monkeypatch.setenv("HFB_TMA_FEED", "0")
+    p2, e2 = run()
+    assert float((p1 - p2).abs().max()) <= 1e-4 * float(p2.abs().max())
+    assert np.max(np.abs(e1 - e2)) < 1e-3
 
 
 def _near_diag_hermitian(n, seed, scale, kramers=True):
