@@ -27,6 +27,7 @@
 // Every wait is bounded; a timeout latches HFB_ERR_CUDA, drains the MMAs
 // in flight and releases TMEM before returning.
 #include <math.h>
+#include <stdlib.h>
 #include "hfb_ctx.cuh"
 #include "tc_sm100.cuh"
 
@@ -53,6 +54,7 @@ struct TcUnit {
 };
 struct TcJob {
   int nunit, kchunks, kb_total, n3;
+  int drain;                      // K blocks accumulated in TMEM between drains
   TcUnit u[kTcMaxUnits];
   int s0[2], ns[2], np[2];
   const double* vp[2];
@@ -191,21 +193,22 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
     if (lane == 0) {
       const uint32_t idesc = tc::idesc_tf32(128, np);
       for (int w = 0; w < nwin; ++w) {
-        const int s = w % kTcStages, d = w & 1;
+        const int s = w % kTcStages, e = w / job.drain, d = e & 1;
+        const bool first = w % job.drain == 0, last = w % job.drain == job.drain - 1 || w == nwin - 1;
         if (!wait(&full[s], (uint32_t)((w / kTcStages) & 1))) break;
-        if (w >= 2 && !wait(&dempty[d], (uint32_t)((w / 2 - 1) & 1))) break;
+        if (first && e >= 2 && !wait(&dempty[d], (uint32_t)((e / 2 - 1) & 1))) break;
         tc::fence_after();
         const uint32_t sa = tc::smem_u32(smem + (size_t)s * sbytes);
         const uint32_t ahi = sa, alo = sa + kTcABytes, bhi = sa + 2 * kTcABytes, blo = bhi + (uint32_t)np * 128;
         const uint32_t dt = tmem + (uint32_t)(d * 256);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          tc::mma_tf32(dt, tc::sw128_desc(ahi + 32 * k), tc::sw128_desc(bhi + 32 * k), idesc, k > 0);
+          tc::mma_tf32(dt, tc::sw128_desc(ahi + 32 * k), tc::sw128_desc(bhi + 32 * k), idesc, k > 0 || !first);
           tc::mma_tf32(dt, tc::sw128_desc(ahi + 32 * k), tc::sw128_desc(blo + 32 * k), idesc, 1);
           tc::mma_tf32(dt, tc::sw128_desc(alo + 32 * k), tc::sw128_desc(bhi + 32 * k), idesc, 1);
         }
         tc::mma_commit(&empty[s]);
-        tc::mma_commit(&dfull[d]);
+        if (last) tc::mma_commit(&dfull[d]);
       }
       // every MMA issued above has completed once this arrives
       tc::mma_commit(&fin);
@@ -224,14 +227,24 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
 #pragma unroll
       for (int i = 0; i < 16; ++i) acc[g][i] = 0.f;
     bool ok = true;
-    for (int w = 0; w < nwin; ++w) {
-      const int d = w & 1;
-      if (!wait(&dfull[d], (uint32_t)((w / 2) & 1))) { ok = false; break; }
+    const int nep = (nwin + job.drain - 1) / job.drain;
+    for (int e = 0; e < nep; ++e) {
+      const int d = e & 1;
+      if (!wait(&dfull[d], (uint32_t)((e / 2) & 1))) { ok = false; break; }
       tc::fence_after();
       const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(d * 256);
+      // two groups per load where possible: fewer load-wait round trips
 #pragma unroll
-      for (int g = 0; g < kTcMaxGroups; ++g) {
-        if (g < gcnt) {
+      for (int g = 0; g < kTcMaxGroups; g += 2) {
+        if (g + 1 < gcnt) {
+          float v[32];
+          tc::tmem_ld32(ta + (uint32_t)((gbeg + g) * 16), v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            acc[g][i] += v[i];
+            acc[g + 1][i] += v[16 + i];
+          }
+        } else if (g < gcnt) {
           float v[16];
           tc::tmem_ld16(ta + (uint32_t)((gbeg + g) * 16), v);
 #pragma unroll
@@ -383,20 +396,21 @@ gram_tma_kernel(TcJob job, const __grid_constant__ CUtensorMap mpsi, const __gri
     if (lane == 0) {
       const uint32_t idesc = tc::idesc_tf32(128, np);
       for (int w = 0; w < nwin; ++w) {
-        const int s = w % kGtStages, d = w & 1;
+        const int s = w % kGtStages, e = w / job.drain, d = e & 1;
+        const bool first = w % job.drain == 0, last = w % job.drain == job.drain - 1 || w == nwin - 1;
         if (!wait(&conv_full[s], (uint32_t)((w / kGtStages) & 1))) break;
-        if (w >= 2 && !wait(&dempty[d], (uint32_t)((w / 2 - 1) & 1))) break;
+        if (first && e >= 2 && !wait(&dempty[d], (uint32_t)((e / 2 - 1) & 1))) break;
         tc::fence_after();
         const uint32_t bhi = tc::smem_u32(smem + (size_t)s * sbytes + kGtRawA), blo = bhi + bbytes;
         const uint32_t dt = tmem + (uint32_t)d * kGtD1, at = tmem + kGtACol + (uint32_t)s * 64;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, k > 0);
+          tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, k > 0 || !first);
           tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(blo + 32 * k), idesc, 1);
           tc::mma_tf32_ta(dt, at + 32 + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, 1);
         }
         tc::mma_commit(&empty[s]);
-        tc::mma_commit(&dfull[d]);
+        if (last) tc::mma_commit(&dfull[d]);
       }
       tc::mma_commit(&fin);
       if (!tc::mbar_wait(&fin, 0, limit)) latch_error(status, HFB_ERR_CUDA);
@@ -480,14 +494,24 @@ gram_tma_kernel(TcJob job, const __grid_constant__ CUtensorMap mpsi, const __gri
 #pragma unroll
       for (int i = 0; i < 16; ++i) acc[g][i] = 0.f;
     bool ok = true;
-    for (int w = 0; w < nwin; ++w) {
-      const int d = w & 1;
-      if (!wait(&dfull[d], (uint32_t)((w / 2) & 1))) { ok = false; break; }
+    const int nep = (nwin + job.drain - 1) / job.drain;
+    for (int e = 0; e < nep; ++e) {
+      const int d = e & 1;
+      if (!wait(&dfull[d], (uint32_t)((e / 2) & 1))) { ok = false; break; }
       tc::fence_after();
       const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)d * kGtD1;
+      // two groups per load where possible: fewer load-wait round trips
 #pragma unroll
-      for (int g = 0; g < kTcMaxGroups; ++g) {
-        if (g < gcnt) {
+      for (int g = 0; g < kTcMaxGroups; g += 2) {
+        if (g + 1 < gcnt) {
+          float v[32];
+          tc::tmem_ld32(ta + (uint32_t)((gbeg + g) * 16), v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            acc[g][i] += v[i];
+            acc[g + 1][i] += v[16 + i];
+          }
+        } else if (g < gcnt) {
           float v[16];
           tc::tmem_ld16(ta + (uint32_t)((gbeg + g) * 16), v);
 #pragma unroll
@@ -584,6 +608,11 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  {
+    const char* e = getenv("HFB_GRAM_DRAIN");
+    job.drain = e ? atoi(e) : 1;
+    if (job.drain < 1) job.drain = 1;
   }
   job.kchunks = nsm / job.nunit;
   if (job.kchunks < 1) job.kchunks = 1;
