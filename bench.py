@@ -65,11 +65,12 @@ REFERENCE_ARM_BUDGET_S = 300.0
 # that the final states also carry converged single-particle energies for
 # the |d e_i| comparison.
 STOP_MEV = 1e-6
-# DRAM bytes (read + write) of one hpsi launch (hpsi_bf3_kernel with its
-# field repack, 236 FP32 states, one output): dram__bytes_read.sum +
-# dram__bytes_write.sum of an ncu capture of the same call (python -m
-# hfb.microbench hpsi); None until captured for this kernel.
-HPSI_NCU_DRAM_BYTES = None
+# DRAM bytes (read + write) of one hpsi call (hpsi_bf3_kernel with its field
+# repack and line means, 236 FP32 states, one output): dram__bytes_read.sum
+# + dram__bytes_write.sum of the three kernels in an ncu capture of the same
+# call (python -m hfb.microbench hpsi; 447.5 + 395.0 MB hpsi_bf3_kernel,
+# 9.7 MB hb_fields_kernel, 0.9 MB hb_bbar_kernel).
+HPSI_NCU_DRAM_BYTES = 853145344
 HPSI_KERNEL = "hpsi (hb_fields_kernel + hb_bbar_kernel + hpsi_bf3_kernel, tcgen05 bf16x3), FP32, 236 states"
 
 

@@ -28,6 +28,7 @@
 // in flight and releases TMEM before returning.
 #include <math.h>
 #include <stdlib.h>
+#include <string.h>
 #include "hfb_ctx.cuh"
 #include "tc_sm100.cuh"
 
@@ -281,9 +282,9 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
 // accelerator and A in tensor memory.
 //
 //   warp 0      (one thread) TMA: the raw fp32 K block of the unit's A'
-//               rows (two row ranges: the Psi part and the Psi~ part, each
-//               in 8-row boxes from an 8-row boundary) and of its B rows,
-//               128-byte swizzled, into a 3-stage ring;
+//               rows (the Psi part and the Psi~ part, one 128-row box each,
+//               at rows 0 and 128 of the stage) and of its B rows (one box
+//               of np rows), 128-byte swizzled, into a 3-stage ring;
 //   warp 1      (one thread) MMAs, A from tensor memory (M = 128, N = np,
 //               K = 8), into one of two accumulators; it owns the TMEM
 //               allocation;
@@ -299,12 +300,20 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
 constexpr int kGtStages = 3;
 constexpr int kGtThreads = 512;
 constexpr int kGtConvWarps = 6;          // warps 2-7
-constexpr uint32_t kGtRawA = 144 * 128;  // A' raw rows: round8(cnt1) + round8(cnt2) <= 142
+constexpr uint32_t kGtRawA = 256 * 128;  // A' raw rows: the Psi part at row 0, the Psi~ part at row 128
+
+// Tensor maps of one launch: A' rows of psi in 128-row boxes, and the B rows
+// of each block and source (psi, hampsi, hmfpsi) in boxes of that block's np
+// rows, so that a K block is three copies at most.
+struct GtMaps {
+  CUtensorMap a;
+  CUtensorMap b[2][3];
+};
 constexpr uint32_t kGtD1 = 160, kGtACol = 320;
 
 __global__ void __launch_bounds__(kGtThreads, 1)
-gram_tma_kernel(TcJob job, const __grid_constant__ CUtensorMap mpsi, const __grid_constant__ CUtensorMap mham,
-                const __grid_constant__ CUtensorMap mhmf, float* __restrict__ part, int* status, long long limit) {
+gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restrict__ part, int* status,
+                long long limit) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ uint64_t raw_full[kGtStages], empty[kGtStages], conv_full[kGtStages], dfull[2], dempty[2], fin;
@@ -325,8 +334,6 @@ gram_tma_kernel(TcJob job, const __grid_constant__ CUtensorMap mpsi, const __gri
   const int g0 = mb * 128;
   const int cnt1 = max(0, min(n, g0 + 128) - g0);
   const int lo2 = max(n, g0), cnt2 = max(0, min(2 * n, g0 + 128) - lo2);
-  const int r2 = (cnt1 + 7) / 8 * 8;
-  const int nbox1 = (cnt1 + 7) / 8, nbox2 = (cnt2 + 7) / 8, nboxb = np / 8;
 
   if (tid == 0) {
     for (int s = 0; s < kGtStages; ++s) {
@@ -368,8 +375,8 @@ gram_tma_kernel(TcJob job, const __grid_constant__ CUtensorMap mpsi, const __gri
   if (warp == 0) {
     // ---------------------------------------------------------------- TMA
     if (lane == 0) {
-      const CUtensorMap* mapb = am == 1 ? &mham : am == 2 ? &mhmf : &mpsi;
-      const uint32_t tx = (uint32_t)(nbox1 + nbox2 + nboxb) * 1024u;
+      const CUtensorMap* mapb = &maps.b[b][am == 1 ? 1 : am == 2 ? 2 : 0];
+      const uint32_t tx = (cnt1 > 0 ? 16384u : 0u) + (cnt2 > 0 ? 16384u : 0u) + bbytes;
       const int p0 = job.s0[b] + g0, t0 = job.s0[b] + lo2 - n, q0 = job.s0[b];
       int issued = 0;
       for (int w = 0; w < nwin; ++w) {
@@ -378,11 +385,9 @@ gram_tma_kernel(TcJob job, const __grid_constant__ CUtensorMap mpsi, const __gri
         unsigned char* st = smem + (size_t)s * sbytes;
         tc::mbar_arrive_expect_tx(&raw_full[s], tx);
         const int x = (kb0 + w) * 32;
-        for (int i = 0; i < nbox1; ++i) tc::tma_load_2d(st + i * 1024, &mpsi, x, p0 + 8 * i, &raw_full[s]);
-        for (int i = 0; i < nbox2; ++i)
-          tc::tma_load_2d(st + (r2 / 8 + i) * 1024, &mpsi, x, t0 + 8 * i, &raw_full[s]);
-        for (int i = 0; i < nboxb; ++i)
-          tc::tma_load_2d(st + kGtRawA + i * 1024, mapb, x, q0 + 8 * i, &raw_full[s]);
+        if (cnt1 > 0) tc::tma_load_2d(st, &maps.a, x, p0, &raw_full[s]);
+        if (cnt2 > 0) tc::tma_load_2d(st + 16384, &maps.a, x, t0, &raw_full[s]);
+        tc::tma_load_2d(st + kGtRawA, mapb, x, q0, &raw_full[s]);
         issued = w + 1;
       }
       // copies still in flight land before the CTA can exit
@@ -427,7 +432,7 @@ gram_tma_kernel(TcJob job, const __grid_constant__ CUtensorMap mpsi, const __gri
     if (r < cnt1) {
       arow = r;
     } else if (r < cnt1 + cnt2) {
-      arow = r2 + (r - cnt1);
+      arow = 128 + (r - cnt1);
       tilde = true;
     }
     for (int w = 0; w < nwin; ++w) {
@@ -628,16 +633,24 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
     int rows = 0;
     for (int b = 0; b < nblk; ++b)
       if (ns[b] > 0) rows = s0[b] + ns[b] > rows ? s0[b] + ns[b] : rows;
-    CUtensorMap mp, mh, mm;
     const uint64_t kf = 4 * (uint64_t)job.n3;
-    if (!encode_fp32_rows_map(&mp, psi, kf, rows, 8)) return HFB_ERR_CUDA;
-    mh = mp;
-    mm = mp;
-    if (hampsi && !encode_fp32_rows_map(&mh, hampsi, kf, rows, 8)) return HFB_ERR_CUDA;
-    if (hmfpsi && !encode_fp32_rows_map(&mm, hmfpsi, kf, rows, 8)) return HFB_ERR_CUDA;
+    GtMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    if (!encode_fp32_rows_map(&maps.a, psi, kf, rows, 128)) return HFB_ERR_CUDA;
+    const void* src[3] = {psi, hampsi, hmfpsi};
+    for (int b = 0; b < nblk; ++b) {
+      if (ns[b] <= 0) continue;
+      for (int j = 0; j < 3; ++j) {
+        bool used = false;
+        for (int a = 0; a < 4; ++a)
+          if ((masks[b] & (1 << a)) && (a == 1 ? 1 : a == 2 ? 2 : 0) == j) used = true;
+        if (used && (!src[j] || !encode_fp32_rows_map(&maps.b[b][j], src[j], kf, rows, job.np[b])))
+          return HFB_ERR_CUDA;
+      }
+    }
     const size_t smem = 1024 + (size_t)kGtStages * (kGtRawA + 2 * (size_t)npmax * 128);
     allow_max_dynamic_smem(gram_tma_kernel);
-    gram_tma_kernel<<<ncta, kGtThreads, smem, st>>>(job, mp, mh, mm, part, c->dev_status, c->wait_limit);
+    gram_tma_kernel<<<ncta, kGtThreads, smem, st>>>(job, maps, part, c->dev_status, c->wait_limit);
   } else {
     const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)npmax * 128);
     allow_max_dynamic_smem(gram_tc_kernel);
