@@ -10,17 +10,20 @@
 // about 22 significant bits per product).
 //
 // One CTA owns one 128-row block of A' for one matrix and one slice of K.
-// Two kernels: gram_tma_kernel (the default, below) and gram_tc_kernel,
-// whose producers load through registers:
+// Two kernels: gram_tc_kernel (the default), whose producers load through
+// registers, and gram_tma_kernel (below; HFB_GRAM_TMA=1), which measured
+// slower on Pb208 (2.99 ms against 2.07 ms for the 140 neutron states):
+// its in-place split of B adds shared-memory traffic to a kernel whose
+// MMAs already read about 100 KB of shared memory per K block.
 //   warps 0-6   load a 32-float K block of the rows from global memory,
 //               split it and store it into a 128-byte-swizzled stage
 //               (3-stage ring);
 //   warp 7      issues the MMAs (M = 128, N = n padded to 16, K = 8) into
-//               one of two TMEM accumulators; each K block is a window that
-//               starts from zero;
-//   warps 8-15  drain the finished accumulator into fp32 registers, so the
-//               tensor core's own fp32 accumulation spans at most one
-//               window (12 MMAs) and the sum over windows is rounded to
+//               one of two TMEM accumulators, which starts from zero every
+//               four K blocks;
+//   warps 8-15  drain the finished accumulator into fp32 registers every
+//               four K blocks, so the tensor core's own fp32 accumulation
+//               spans at most 48 MMAs and the sum over drains is rounded to
 //               nearest.
 // Per-slice partial sums are added in fp64 in a fixed order by a second
 // kernel, which also scatters Re/Im rows into the complex outputs.
@@ -49,6 +52,7 @@ constexpr int kTcItemsB = (kTcMaxNp + kTcRowsPerPass - 1) / kTcRowsPerPass;
 constexpr int kTcTmemCols = 512;        // two accumulators at columns 0 and 256
 constexpr uint32_t kTcABytes = 128 * 128;   // 128 rows x 128 bytes
 constexpr long long kTcWaitLimit = 2000000000LL;
+constexpr int kTcDrain = 4;
 
 struct TcUnit {
   unsigned char b, a, mb, pad;
@@ -615,8 +619,11 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   }
   {
+    // K blocks accumulated in TMEM between drains into registers: 4
+    // measured 6 % faster than 1 on Pb208 and stays inside the 3e-6 bar of
+    // the single-precision Gram test; HFB_GRAM_DRAIN overrides
     const char* e = getenv("HFB_GRAM_DRAIN");
-    job.drain = e ? atoi(e) : 1;
+    job.drain = e ? atoi(e) : kTcDrain;
     if (job.drain < 1) job.drain = 1;
   }
   job.kchunks = nsm / job.nunit;
@@ -627,7 +634,7 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
   if (!part) return HFB_ERR_ALLOC;
   int npmax = 16;
   for (int b = 0; b < nblk; ++b) npmax = job.np[b] > npmax ? job.np[b] : npmax;
-  if (c->tma_feed) {
+  if (c->gram_tma) {
     // tensor maps over the states as rows of 4 n^3 floats (both spin
     // components, interleaved re/im), rows up to the last state used
     int rows = 0;
