@@ -283,32 +283,34 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
 
 // ---------------------------------------------------------------------------
 // The same products with the K blocks brought in by the tensor-memory
-// accelerator and A in tensor memory.
+// accelerator and A in tensor memory.  Two rings: the raw blocks the TMA
+// lands (kGtRawMax stages, as many as shared memory holds) and the split
+// B operands the MMAs read (two stages), so the copies run several K blocks
+// ahead of the splitting, which runs up to two ahead of the MMAs.
 //
 //   warp 0      (one thread) TMA: the raw fp32 K block of the unit's A'
-//               rows (the Psi part and the Psi~ part, one 128-row box each,
-//               at rows 0 and 128 of the stage) and of its B rows (one box
-//               of np rows), 128-byte swizzled, into a 3-stage ring;
+//               rows (the Psi part and the Psi~ part, each in 8-row boxes
+//               from an 8-row boundary, the second part after the first)
+//               and of its B rows (one box of np rows), 128-byte swizzled;
 //   warp 1      (one thread) MMAs, A from tensor memory (M = 128, N = np,
 //               K = 8), into one of two accumulators; it owns the TMEM
 //               allocation;
-//   warps 2-7   split B in place (hi over the raw block, lo beside it; rows
-//               past n zeroed, v_pair applied for the fourth matrix);
+//   warps 2-7   split B from the raw block into the operand stage (hi and
+//               lo; rows past n zeroed, v_pair applied for the fourth
+//               matrix);
 //   warps 4-7   also split A' (one row per thread, Psi~ rows formed as
-//               (-im, re)) and store hi and lo into the stage's 64 TMEM
-//               columns;
+//               (-im, re)) into the operand stage's 64 TMEM columns;
 //   warps 8-15  drain the accumulators as in gram_tc_kernel.
-// TMEM: accumulators at columns 0 and 160, A stages at 320 + 64 s.  A stage
-// of shared memory is free again when the MMAs that read it commit, which
-// also frees its TMEM A columns.
-constexpr int kGtStages = 3;
+// TMEM: accumulators at columns 0 and 160, A stages at 320 + 64 o.
+constexpr int kGtRawMax = 6;
+constexpr int kGtOpStages = 2;
 constexpr int kGtThreads = 512;
 constexpr int kGtConvWarps = 6;          // warps 2-7
-constexpr uint32_t kGtRawA = 256 * 128;  // A' raw rows: the Psi part at row 0, the Psi~ part at row 128
+constexpr uint32_t kGtRawA = 144 * 128;  // A' raw rows: round8(cnt1) + round8(cnt2) <= 142
 
-// Tensor maps of one launch: A' rows of psi in 128-row boxes, and the B rows
-// of each block and source (psi, hampsi, hmfpsi) in boxes of that block's np
-// rows, so that a K block is three copies at most.
+// Tensor maps of one launch: the A' rows of psi in 8-row boxes, and the B
+// rows of each block and source (psi, hampsi, hmfpsi) in boxes of that
+// block's np rows.
 struct GtMaps {
   CUtensorMap a;
   CUtensorMap b[2][3];
@@ -317,10 +319,11 @@ constexpr uint32_t kGtD1 = 160, kGtACol = 320;
 
 __global__ void __launch_bounds__(kGtThreads, 1)
 gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restrict__ part, int* status,
-                long long limit) {
+                long long limit, int nraw) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ uint64_t raw_full[kGtStages], empty[kGtStages], conv_full[kGtStages], dfull[2], dempty[2], fin;
+  __shared__ uint64_t raw_full[kGtRawMax], raw_empty[kGtRawMax], op_full[kGtOpStages], op_empty[kGtOpStages];
+  __shared__ uint64_t dfull[2], dempty[2], fin;
   __shared__ uint32_t tbase;
   __shared__ volatile int abort_flag;
 
@@ -331,19 +334,25 @@ gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restric
   const int kb0 = (int)((long long)job.kb_total * chunk / job.kchunks);
   const int kb1 = (int)((long long)job.kb_total * (chunk + 1) / job.kchunks);
   const int nwin = kb1 - kb0;
-  const uint32_t bbytes = (uint32_t)np * 128, sbytes = kGtRawA + 2 * bbytes;
+  const uint32_t bbytes = (uint32_t)np * 128, rbytes = kGtRawA + bbytes, obytes = 2 * bbytes;
+  unsigned char* ops = smem + (size_t)nraw * rbytes;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid & 31;
   // A' rows g0 .. g0 + 127: Psi rows of states g0 .. (cnt1 of them), then
   // Psi~ rows of states lo2 - n .. (cnt2 of them)
   const int g0 = mb * 128;
   const int cnt1 = max(0, min(n, g0 + 128) - g0);
   const int lo2 = max(n, g0), cnt2 = max(0, min(2 * n, g0 + 128) - lo2);
+  const int r2 = (cnt1 + 7) / 8 * 8;
+  const int nbox1 = (cnt1 + 7) / 8, nbox2 = (cnt2 + 7) / 8;
 
   if (tid == 0) {
-    for (int s = 0; s < kGtStages; ++s) {
-      tc::mbar_init(&raw_full[s], 1);
-      tc::mbar_init(&empty[s], 1);
-      tc::mbar_init(&conv_full[s], kGtConvWarps);
+    for (int r = 0; r < nraw; ++r) {
+      tc::mbar_init(&raw_full[r], 1);
+      tc::mbar_init(&raw_empty[r], kGtConvWarps);
+    }
+    for (int o = 0; o < kGtOpStages; ++o) {
+      tc::mbar_init(&op_full[o], kGtConvWarps);
+      tc::mbar_init(&op_empty[o], 1);
     }
     for (int d = 0; d < 2; ++d) {
       tc::mbar_init(&dfull[d], 1);
@@ -380,24 +389,24 @@ gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restric
     // ---------------------------------------------------------------- TMA
     if (lane == 0) {
       const CUtensorMap* mapb = &maps.b[b][am == 1 ? 1 : am == 2 ? 2 : 0];
-      const uint32_t tx = (cnt1 > 0 ? 16384u : 0u) + (cnt2 > 0 ? 16384u : 0u) + bbytes;
+      const uint32_t tx = (uint32_t)(nbox1 + nbox2) * 1024u + bbytes;
       const int p0 = job.s0[b] + g0, t0 = job.s0[b] + lo2 - n, q0 = job.s0[b];
       int issued = 0;
       for (int w = 0; w < nwin; ++w) {
-        const int s = w % kGtStages;
-        if (w >= kGtStages && !wait(&empty[s], (uint32_t)((w / kGtStages - 1) & 1))) break;
-        unsigned char* st = smem + (size_t)s * sbytes;
-        tc::mbar_arrive_expect_tx(&raw_full[s], tx);
+        const int r = w % nraw;
+        if (w >= nraw && !wait(&raw_empty[r], (uint32_t)((w / nraw - 1) & 1))) break;
+        unsigned char* st = smem + (size_t)r * rbytes;
+        tc::mbar_arrive_expect_tx(&raw_full[r], tx);
         const int x = (kb0 + w) * 32;
-        if (cnt1 > 0) tc::tma_load_2d(st, &maps.a, x, p0, &raw_full[s]);
-        if (cnt2 > 0) tc::tma_load_2d(st + 16384, &maps.a, x, t0, &raw_full[s]);
-        tc::tma_load_2d(st + kGtRawA, mapb, x, q0, &raw_full[s]);
+        for (int i = 0; i < nbox1; ++i) tc::tma_load_2d(st + i * 1024, &maps.a, x, p0 + 8 * i, &raw_full[r]);
+        for (int i = 0; i < nbox2; ++i)
+          tc::tma_load_2d(st + (r2 / 8 + i) * 1024, &maps.a, x, t0 + 8 * i, &raw_full[r]);
+        tc::tma_load_2d(st + kGtRawA, mapb, x, q0, &raw_full[r]);
         issued = w + 1;
       }
       // copies still in flight land before the CTA can exit
-      for (int w = max(0, issued - kGtStages); w < issued; ++w)
-        if (!tc::mbar_wait(&raw_full[w % kGtStages], (uint32_t)((w / kGtStages) & 1), limit))
-          latch_error(status, HFB_ERR_CUDA);
+      for (int w = max(0, issued - nraw); w < issued; ++w)
+        if (!tc::mbar_wait(&raw_full[w % nraw], (uint32_t)((w / nraw) & 1), limit)) latch_error(status, HFB_ERR_CUDA);
     }
     __syncwarp();
   } else if (warp == 1) {
@@ -405,20 +414,20 @@ gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restric
     if (lane == 0) {
       const uint32_t idesc = tc::idesc_tf32(128, np);
       for (int w = 0; w < nwin; ++w) {
-        const int s = w % kGtStages, e = w / job.drain, d = e & 1;
+        const int o = w % kGtOpStages, e = w / job.drain, d = e & 1;
         const bool first = w % job.drain == 0, last = w % job.drain == job.drain - 1 || w == nwin - 1;
-        if (!wait(&conv_full[s], (uint32_t)((w / kGtStages) & 1))) break;
+        if (!wait(&op_full[o], (uint32_t)((w / kGtOpStages) & 1))) break;
         if (first && e >= 2 && !wait(&dempty[d], (uint32_t)((e / 2 - 1) & 1))) break;
         tc::fence_after();
-        const uint32_t bhi = tc::smem_u32(smem + (size_t)s * sbytes + kGtRawA), blo = bhi + bbytes;
-        const uint32_t dt = tmem + (uint32_t)d * kGtD1, at = tmem + kGtACol + (uint32_t)s * 64;
+        const uint32_t bhi = tc::smem_u32(ops + (size_t)o * obytes), blo = bhi + bbytes;
+        const uint32_t dt = tmem + (uint32_t)d * kGtD1, at = tmem + kGtACol + (uint32_t)o * 64;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, k > 0 || !first);
           tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(blo + 32 * k), idesc, 1);
           tc::mma_tf32_ta(dt, at + 32 + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, 1);
         }
-        tc::mma_commit(&empty[s]);
+        tc::mma_commit(&op_empty[o]);
         if (last) tc::mma_commit(&dfull[d]);
       }
       tc::mma_commit(&fin);
@@ -436,19 +445,21 @@ gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restric
     if (r < cnt1) {
       arow = r;
     } else if (r < cnt1 + cnt2) {
-      arow = 128 + (r - cnt1);
+      arow = r2 + (r - cnt1);
       tilde = true;
     }
     for (int w = 0; w < nwin; ++w) {
-      const int s = w % kGtStages;
-      if (!wait(&raw_full[s], (uint32_t)((w / kGtStages) & 1))) break;
-      unsigned char* st = smem + (size_t)s * sbytes;
-      unsigned char* bh = st + kGtRawA;
+      const int rs = w % nraw, o = w % kGtOpStages;
+      if (!wait(&raw_full[rs], (uint32_t)((w / nraw) & 1))) break;
+      if (w >= kGtOpStages && !wait(&op_empty[o], (uint32_t)((w / kGtOpStages - 1) & 1))) break;
+      const unsigned char* st = smem + (size_t)rs * rbytes;
+      const unsigned char* bs = st + kGtRawA;
+      unsigned char* oh = ops + (size_t)o * obytes;
       const size_t xoff = (size_t)(kb0 + w) * 32;
       for (int e = ct; e < np * 8; e += kGtConvWarps * 32) {
         const int row = e >> 3, c = e & 7;
-        const uint32_t o = tc::sw128_offset(row, c);
-        float4 v = *reinterpret_cast<const float4*>(bh + o);
+        const uint32_t off = tc::sw128_offset(row, c);
+        float4 v = *reinterpret_cast<const float4*>(bs + off);
         if (row >= n) {
           v = make_float4(0.f, 0.f, 0.f, 0.f);
         } else if (am == 3) {
@@ -461,11 +472,11 @@ gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restric
         h.y = tc::to_tf32(v.y); l.y = tc::to_tf32(v.y - h.y);
         h.z = tc::to_tf32(v.z); l.z = tc::to_tf32(v.z - h.z);
         h.w = tc::to_tf32(v.w); l.w = tc::to_tf32(v.w - h.w);
-        *reinterpret_cast<float4*>(bh + o) = h;
-        *reinterpret_cast<float4*>(bh + bbytes + o) = l;
+        *reinterpret_cast<float4*>(oh + off) = h;
+        *reinterpret_cast<float4*>(oh + bbytes + off) = l;
       }
       if (do_a) {
-        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + kGtACol + (uint32_t)s * 64;
+        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + kGtACol + (uint32_t)o * 64;
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
           float hv[16], lv[16];
@@ -489,7 +500,10 @@ gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restric
       tc::fence_proxy_async_smem();
       tc::fence_before();
       __syncwarp();
-      if (lane == 0) tc::mbar_arrive(&conv_full[s]);
+      if (lane == 0) {
+        tc::mbar_arrive(&raw_empty[rs]);
+        tc::mbar_arrive(&op_full[o]);
+      }
     }
   } else {
     // ----------------------------------------------------------- epilogue
@@ -509,7 +523,6 @@ gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restric
       if (!wait(&dfull[d], (uint32_t)((e / 2) & 1))) { ok = false; break; }
       tc::fence_after();
       const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)d * kGtD1;
-      // two groups per load where possible: fewer load-wait round trips
 #pragma unroll
       for (int g = 0; g < kTcMaxGroups; g += 2) {
         if (g + 1 < gcnt) {
@@ -643,7 +656,7 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
     const uint64_t kf = 4 * (uint64_t)job.n3;
     GtMaps maps;
     memset(&maps, 0, sizeof(maps));
-    if (!encode_fp32_rows_map(&maps.a, psi, kf, rows, 128)) return HFB_ERR_CUDA;
+    if (!encode_fp32_rows_map(&maps.a, psi, kf, rows, 8)) return HFB_ERR_CUDA;
     const void* src[3] = {psi, hampsi, hmfpsi};
     for (int b = 0; b < nblk; ++b) {
       if (ns[b] <= 0) continue;
@@ -655,9 +668,22 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
           return HFB_ERR_CUDA;
       }
     }
-    const size_t smem = 1024 + (size_t)kGtStages * (kGtRawA + 2 * (size_t)npmax * 128);
+    // raw stages: as many as the shared memory left by the two operand
+    // stages holds (3 to kGtRawMax)
+    int optin = 0;
+    {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    }
+    const size_t rb = kGtRawA + (size_t)npmax * 128, ob = 2 * (size_t)npmax * 128;
+    const size_t avail = (size_t)optin - 1024 - 1024 - kGtOpStages * ob;
+    int nraw = (int)(avail / rb);
+    if (nraw > kGtRawMax) nraw = kGtRawMax;
+    if (nraw < 3) return HFB_ERR_UNSUPPORTED_GRID;
+    const size_t smem = 1024 + (size_t)nraw * rb + kGtOpStages * ob;
     allow_max_dynamic_smem(gram_tma_kernel);
-    gram_tma_kernel<<<ncta, kGtThreads, smem, st>>>(job, maps, part, c->dev_status, c->wait_limit);
+    gram_tma_kernel<<<ncta, kGtThreads, smem, st>>>(job, maps, part, c->dev_status, c->wait_limit, nraw);
   } else {
     const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)npmax * 128);
     allow_max_dynamic_smem(gram_tc_kernel);
