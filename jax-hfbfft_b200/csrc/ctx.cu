@@ -130,12 +130,9 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     // FP64 Gram and rotation on the FP64 tensor cores unless HFB_F64_MMA=0
     const char* gk = getenv("HFB_F64_MMA");
     c->f64_mma = (gk && gk[0] == '0') ? 0 : 1;
-    // single-precision rotation fed by TMA unless HFB_TMA_FEED=0; the Gram
-    // only with HFB_GRAM_TMA=1
+    // single-precision rotation fed by TMA unless HFB_TMA_FEED=0
     const char* gt = getenv("HFB_TMA_FEED");
     c->tma_feed = (gt && gt[0] == '0') ? 0 : 1;
-    const char* gg = getenv("HFB_GRAM_TMA");
-    c->gram_tma = (gg && gg[0] == '1') ? 1 : 0;
     c->wait_limit = kDefaultWaitLimit;
     c->timeout_probe = 0;
   }

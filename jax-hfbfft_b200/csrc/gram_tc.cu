@@ -10,11 +10,11 @@
 // about 22 significant bits per product).
 //
 // One CTA owns one 128-row block of A' for one matrix and one slice of K.
-// Two kernels: gram_tc_kernel (the default), whose producers load through
-// registers, and gram_tma_kernel (below; HFB_GRAM_TMA=1), which measured
-// slower on Pb208 (2.99 ms against 2.07 ms for the 140 neutron states):
-// its in-place split of B adds shared-memory traffic to a kernel whose
-// MMAs already read about 100 KB of shared memory per K block.
+// (Feeding the K blocks by TMA, with A split into tensor memory as the
+// rotation does, measured slower here: 2.9-3.2 ms against 2.0 ms for the
+// 140 Pb208 neutron states, with 8-row or 128-row boxes and with a deeper
+// raw ring; the split of B then sits on six warps instead of seven, four
+// of which also split A.)
 //   warps 0-6   load a 32-float K block of the rows from global memory,
 //               split it and store it into a 128-byte-swizzled stage
 //               (3-stage ring);
@@ -30,8 +30,6 @@
 // Every wait is bounded; a timeout latches HFB_ERR_CUDA, drains the MMAs
 // in flight and releases TMEM before returning.
 #include <math.h>
-#include <stdlib.h>
-#include <string.h>
 #include "hfb_ctx.cuh"
 #include "tc_sm100.cuh"
 
@@ -52,6 +50,9 @@ constexpr int kTcItemsB = (kTcMaxNp + kTcRowsPerPass - 1) / kTcRowsPerPass;
 constexpr int kTcTmemCols = 512;        // two accumulators at columns 0 and 256
 constexpr uint32_t kTcABytes = 128 * 128;   // 128 rows x 128 bytes
 constexpr long long kTcWaitLimit = 2000000000LL;
+// K blocks accumulated in TMEM between drains into registers: 4 measured
+// 6 % faster than 1 on Pb208 (1.96 ms against 2.09 ms for the 140 neutron
+// states) and stays inside the 3e-6 bar of the single-precision Gram test
 constexpr int kTcDrain = 4;
 
 struct TcUnit {
@@ -281,290 +282,6 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
   }
 }
 
-// ---------------------------------------------------------------------------
-// The same products with the K blocks brought in by the tensor-memory
-// accelerator and A in tensor memory.  Two rings: the raw blocks the TMA
-// lands (kGtRawMax stages, as many as shared memory holds) and the split
-// B operands the MMAs read (two stages), so the copies run several K blocks
-// ahead of the splitting, which runs up to two ahead of the MMAs.
-//
-//   warp 0      (one thread) TMA: the raw fp32 K block of the unit's A'
-//               rows (the Psi part and the Psi~ part, each in 8-row boxes
-//               from an 8-row boundary, the second part after the first)
-//               and of its B rows (one box of np rows), 128-byte swizzled;
-//   warp 1      (one thread) MMAs, A from tensor memory (M = 128, N = np,
-//               K = 8), into one of two accumulators; it owns the TMEM
-//               allocation;
-//   warps 2-7   split B from the raw block into the operand stage (hi and
-//               lo; rows past n zeroed, v_pair applied for the fourth
-//               matrix);
-//   warps 4-7   also split A' (one row per thread, Psi~ rows formed as
-//               (-im, re)) into the operand stage's 64 TMEM columns;
-//   warps 8-15  drain the accumulators as in gram_tc_kernel.
-// TMEM: accumulators at columns 0 and 160, A stages at 320 + 64 o.
-constexpr int kGtRawMax = 6;
-constexpr int kGtOpStages = 2;
-constexpr int kGtThreads = 512;
-constexpr int kGtConvWarps = 6;          // warps 2-7
-constexpr uint32_t kGtRawA = 144 * 128;  // A' raw rows: round8(cnt1) + round8(cnt2) <= 142
-
-// Tensor maps of one launch: the A' rows of psi in 8-row boxes, and the B
-// rows of each block and source (psi, hampsi, hmfpsi) in boxes of that
-// block's np rows.
-struct GtMaps {
-  CUtensorMap a;
-  CUtensorMap b[2][3];
-};
-constexpr uint32_t kGtD1 = 160, kGtACol = 320;
-
-__global__ void __launch_bounds__(kGtThreads, 1)
-gram_tma_kernel(TcJob job, const __grid_constant__ GtMaps maps, float* __restrict__ part, int* status,
-                long long limit, int nraw) {
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ uint64_t raw_full[kGtRawMax], raw_empty[kGtRawMax], op_full[kGtOpStages], op_empty[kGtOpStages];
-  __shared__ uint64_t dfull[2], dempty[2], fin;
-  __shared__ uint32_t tbase;
-  __shared__ volatile int abort_flag;
-
-  const int unit = blockIdx.x % job.nunit, chunk = blockIdx.x / job.nunit;
-  const TcUnit U = job.u[unit];
-  const int b = U.b, am = U.a, mb = U.mb;
-  const int n = job.ns[b], np = job.np[b];
-  const int kb0 = (int)((long long)job.kb_total * chunk / job.kchunks);
-  const int kb1 = (int)((long long)job.kb_total * (chunk + 1) / job.kchunks);
-  const int nwin = kb1 - kb0;
-  const uint32_t bbytes = (uint32_t)np * 128, rbytes = kGtRawA + bbytes, obytes = 2 * bbytes;
-  unsigned char* ops = smem + (size_t)nraw * rbytes;
-  const int tid = threadIdx.x, warp = tid / 32, lane = tid & 31;
-  // A' rows g0 .. g0 + 127: Psi rows of states g0 .. (cnt1 of them), then
-  // Psi~ rows of states lo2 - n .. (cnt2 of them)
-  const int g0 = mb * 128;
-  const int cnt1 = max(0, min(n, g0 + 128) - g0);
-  const int lo2 = max(n, g0), cnt2 = max(0, min(2 * n, g0 + 128) - lo2);
-  const int r2 = (cnt1 + 7) / 8 * 8;
-  const int nbox1 = (cnt1 + 7) / 8, nbox2 = (cnt2 + 7) / 8;
-
-  if (tid == 0) {
-    for (int r = 0; r < nraw; ++r) {
-      tc::mbar_init(&raw_full[r], 1);
-      tc::mbar_init(&raw_empty[r], kGtConvWarps);
-    }
-    for (int o = 0; o < kGtOpStages; ++o) {
-      tc::mbar_init(&op_full[o], kGtConvWarps);
-      tc::mbar_init(&op_empty[o], 1);
-    }
-    for (int d = 0; d < 2; ++d) {
-      tc::mbar_init(&dfull[d], 1);
-      tc::mbar_init(&dempty[d], kTcEpilogueWarps);
-    }
-    tc::mbar_init(&fin, 1);
-    abort_flag = 0;
-  }
-  if (warp == 1) {
-    tc::tmem_alloc(&tbase, kTcTmemCols);
-    tc::tmem_relinquish();
-  }
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  tc::fence_before();
-  __syncthreads();
-  tc::fence_after();
-  const uint32_t tmem = tbase;
-
-  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
-    if (tc::mbar_try_wait(bar, parity)) return true;
-    const long long t0 = clock64();
-    while (!tc::mbar_try_wait(bar, parity)) {
-      if (abort_flag) return false;
-      if (clock64() - t0 > limit) {
-        abort_flag = 1;
-        latch_error(status, HFB_ERR_CUDA);
-        return false;
-      }
-    }
-    return true;
-  };
-
-  if (warp == 0) {
-    // ---------------------------------------------------------------- TMA
-    if (lane == 0) {
-      const CUtensorMap* mapb = &maps.b[b][am == 1 ? 1 : am == 2 ? 2 : 0];
-      const uint32_t tx = (uint32_t)(nbox1 + nbox2) * 1024u + bbytes;
-      const int p0 = job.s0[b] + g0, t0 = job.s0[b] + lo2 - n, q0 = job.s0[b];
-      int issued = 0;
-      for (int w = 0; w < nwin; ++w) {
-        const int r = w % nraw;
-        if (w >= nraw && !wait(&raw_empty[r], (uint32_t)((w / nraw - 1) & 1))) break;
-        unsigned char* st = smem + (size_t)r * rbytes;
-        tc::mbar_arrive_expect_tx(&raw_full[r], tx);
-        const int x = (kb0 + w) * 32;
-        for (int i = 0; i < nbox1; ++i) tc::tma_load_2d(st + i * 1024, &maps.a, x, p0 + 8 * i, &raw_full[r]);
-        for (int i = 0; i < nbox2; ++i)
-          tc::tma_load_2d(st + (r2 / 8 + i) * 1024, &maps.a, x, t0 + 8 * i, &raw_full[r]);
-        tc::tma_load_2d(st + kGtRawA, mapb, x, q0, &raw_full[r]);
-        issued = w + 1;
-      }
-      // copies still in flight land before the CTA can exit
-      for (int w = max(0, issued - nraw); w < issued; ++w)
-        if (!tc::mbar_wait(&raw_full[w % nraw], (uint32_t)((w / nraw) & 1), limit)) latch_error(status, HFB_ERR_CUDA);
-    }
-    __syncwarp();
-  } else if (warp == 1) {
-    // ---------------------------------------------------------------- MMA
-    if (lane == 0) {
-      const uint32_t idesc = tc::idesc_tf32(128, np);
-      for (int w = 0; w < nwin; ++w) {
-        const int o = w % kGtOpStages, e = w / job.drain, d = e & 1;
-        const bool first = w % job.drain == 0, last = w % job.drain == job.drain - 1 || w == nwin - 1;
-        if (!wait(&op_full[o], (uint32_t)((w / kGtOpStages) & 1))) break;
-        if (first && e >= 2 && !wait(&dempty[d], (uint32_t)((e / 2 - 1) & 1))) break;
-        tc::fence_after();
-        const uint32_t bhi = tc::smem_u32(ops + (size_t)o * obytes), blo = bhi + bbytes;
-        const uint32_t dt = tmem + (uint32_t)d * kGtD1, at = tmem + kGtACol + (uint32_t)o * 64;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, k > 0 || !first);
-          tc::mma_tf32_ta(dt, at + 8 * k, tc::sw128_desc(blo + 32 * k), idesc, 1);
-          tc::mma_tf32_ta(dt, at + 32 + 8 * k, tc::sw128_desc(bhi + 32 * k), idesc, 1);
-        }
-        tc::mma_commit(&op_empty[o]);
-        if (last) tc::mma_commit(&dfull[d]);
-      }
-      tc::mma_commit(&fin);
-      if (!tc::mbar_wait(&fin, 0, limit)) latch_error(status, HFB_ERR_CUDA);
-    }
-    __syncwarp();
-  } else if (warp < 8) {
-    // --------------------------------------------------------- converters
-    const int ct = tid - 64;
-    const double* vp = job.vp[b];
-    const int q = warp & 3, r = 32 * q + lane;   // A' row of this thread (warps 4-7)
-    const bool do_a = warp >= 4;
-    int arow = -1;
-    bool tilde = false;
-    if (r < cnt1) {
-      arow = r;
-    } else if (r < cnt1 + cnt2) {
-      arow = r2 + (r - cnt1);
-      tilde = true;
-    }
-    for (int w = 0; w < nwin; ++w) {
-      const int rs = w % nraw, o = w % kGtOpStages;
-      if (!wait(&raw_full[rs], (uint32_t)((w / nraw) & 1))) break;
-      if (w >= kGtOpStages && !wait(&op_empty[o], (uint32_t)((w / kGtOpStages - 1) & 1))) break;
-      const unsigned char* st = smem + (size_t)rs * rbytes;
-      const unsigned char* bs = st + kGtRawA;
-      unsigned char* oh = ops + (size_t)o * obytes;
-      const size_t xoff = (size_t)(kb0 + w) * 32;
-      for (int e = ct; e < np * 8; e += kGtConvWarps * 32) {
-        const int row = e >> 3, c = e & 7;
-        const uint32_t off = tc::sw128_offset(row, c);
-        float4 v = *reinterpret_cast<const float4*>(bs + off);
-        if (row >= n) {
-          v = make_float4(0.f, 0.f, 0.f, 0.f);
-        } else if (am == 3) {
-          const size_t k = ((xoff + 4 * c) / 2) % (size_t)job.n3;
-          const float v0 = (float)vp[k], v1 = (float)vp[k + 1];
-          v = make_float4(v0 * v.x, v0 * v.y, v1 * v.z, v1 * v.w);
-        }
-        float4 h, l;
-        h.x = tc::to_tf32(v.x); l.x = tc::to_tf32(v.x - h.x);
-        h.y = tc::to_tf32(v.y); l.y = tc::to_tf32(v.y - h.y);
-        h.z = tc::to_tf32(v.z); l.z = tc::to_tf32(v.z - h.z);
-        h.w = tc::to_tf32(v.w); l.w = tc::to_tf32(v.w - h.w);
-        *reinterpret_cast<float4*>(oh + off) = h;
-        *reinterpret_cast<float4*>(oh + bbytes + off) = l;
-      }
-      if (do_a) {
-        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + kGtACol + (uint32_t)o * 64;
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-          float hv[16], lv[16];
-#pragma unroll
-          for (int c4 = 0; c4 < 4; ++c4) {
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (arow >= 0) v = *reinterpret_cast<const float4*>(st + tc::sw128_offset(arow, 4 * half + c4));
-            if (tilde) v = make_float4(-v.y, v.x, -v.w, v.z);
-            const float x4[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              hv[4 * c4 + i] = tc::to_tf32(x4[i]);
-              lv[4 * c4 + i] = tc::to_tf32(x4[i] - hv[4 * c4 + i]);
-            }
-          }
-          tc::tmem_st16(ta + 16 * half, hv);
-          tc::tmem_st16(ta + 32 + 16 * half, lv);
-        }
-        tc::tmem_st_wait();
-      }
-      tc::fence_proxy_async_smem();
-      tc::fence_before();
-      __syncwarp();
-      if (lane == 0) {
-        tc::mbar_arrive(&raw_empty[rs]);
-        tc::mbar_arrive(&op_full[o]);
-      }
-    }
-  } else {
-    // ----------------------------------------------------------- epilogue
-    const int q = warp & 3;
-    const int half = (warp - 8) / 4;
-    const int ng = np / 16, gh = (ng + 1) / 2;
-    const int gbeg = half ? gh : 0, gcnt = half ? ng - gh : gh;
-    float acc[kTcMaxGroups][16];
-#pragma unroll
-    for (int g = 0; g < kTcMaxGroups; ++g)
-#pragma unroll
-      for (int i = 0; i < 16; ++i) acc[g][i] = 0.f;
-    bool ok = true;
-    const int nep = (nwin + job.drain - 1) / job.drain;
-    for (int e = 0; e < nep; ++e) {
-      const int d = e & 1;
-      if (!wait(&dfull[d], (uint32_t)((e / 2) & 1))) { ok = false; break; }
-      tc::fence_after();
-      const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)d * kGtD1;
-#pragma unroll
-      for (int g = 0; g < kTcMaxGroups; g += 2) {
-        if (g + 1 < gcnt) {
-          float v[32];
-          tc::tmem_ld32(ta + (uint32_t)((gbeg + g) * 16), v);
-#pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            acc[g][i] += v[i];
-            acc[g + 1][i] += v[16 + i];
-          }
-        } else if (g < gcnt) {
-          float v[16];
-          tc::tmem_ld16(ta + (uint32_t)((gbeg + g) * 16), v);
-#pragma unroll
-          for (int i = 0; i < 16; ++i) acc[g][i] += v[i];
-        }
-      }
-      tc::fence_before();
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(&dempty[d]);
-    }
-    if (ok && !abort_flag) {
-      const int row = q * 32 + lane;
-      float* o = part + ((size_t)blockIdx.x * 128 + row) * kTcMaxNp;
-#pragma unroll
-      for (int g = 0; g < kTcMaxGroups; ++g)
-        if (g < gcnt) {
-#pragma unroll
-          for (int i = 0; i < 16; i += 4)
-            *reinterpret_cast<float4*>(o + (gbeg + g) * 16 + i) =
-                make_float4(acc[g][i], acc[g][i + 1], acc[g][i + 2], acc[g][i + 3]);
-        }
-    }
-  }
-  tc::fence_before();
-  __syncthreads();
-  if (warp == 1) {
-    tc::fence_after();
-    tc::tmem_dealloc(tmem, kTcTmemCols);
-  }
-}
-
 struct TcOut {
   double2* p[8];   // [block * 4 + matrix]
 };
@@ -631,14 +348,7 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   }
-  {
-    // K blocks accumulated in TMEM between drains into registers: 4
-    // measured 6 % faster than 1 on Pb208 and stays inside the 3e-6 bar of
-    // the single-precision Gram test; HFB_GRAM_DRAIN overrides
-    const char* e = getenv("HFB_GRAM_DRAIN");
-    job.drain = e ? atoi(e) : kTcDrain;
-    if (job.drain < 1) job.drain = 1;
-  }
+  job.drain = kTcDrain;
   job.kchunks = nsm / job.nunit;
   if (job.kchunks < 1) job.kchunks = 1;
   if (job.kchunks > job.kb_total) job.kchunks = job.kb_total;
@@ -647,49 +357,10 @@ int gram_tc_launch(hfb_ctx_s* c, int nblk, const int* s0, const int* ns, const i
   if (!part) return HFB_ERR_ALLOC;
   int npmax = 16;
   for (int b = 0; b < nblk; ++b) npmax = job.np[b] > npmax ? job.np[b] : npmax;
-  if (c->gram_tma) {
-    // tensor maps over the states as rows of 4 n^3 floats (both spin
-    // components, interleaved re/im), rows up to the last state used
-    int rows = 0;
-    for (int b = 0; b < nblk; ++b)
-      if (ns[b] > 0) rows = s0[b] + ns[b] > rows ? s0[b] + ns[b] : rows;
-    const uint64_t kf = 4 * (uint64_t)job.n3;
-    GtMaps maps;
-    memset(&maps, 0, sizeof(maps));
-    if (!encode_fp32_rows_map(&maps.a, psi, kf, rows, 8)) return HFB_ERR_CUDA;
-    const void* src[3] = {psi, hampsi, hmfpsi};
-    for (int b = 0; b < nblk; ++b) {
-      if (ns[b] <= 0) continue;
-      for (int j = 0; j < 3; ++j) {
-        bool used = false;
-        for (int a = 0; a < 4; ++a)
-          if ((masks[b] & (1 << a)) && (a == 1 ? 1 : a == 2 ? 2 : 0) == j) used = true;
-        if (used && (!src[j] || !encode_fp32_rows_map(&maps.b[b][j], src[j], kf, rows, job.np[b])))
-          return HFB_ERR_CUDA;
-      }
-    }
-    // raw stages: as many as the shared memory left by the two operand
-    // stages holds (3 to kGtRawMax)
-    int optin = 0;
-    {
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    }
-    const size_t rb = kGtRawA + (size_t)npmax * 128, ob = 2 * (size_t)npmax * 128;
-    const size_t avail = (size_t)optin - 1024 - 1024 - kGtOpStages * ob;
-    int nraw = (int)(avail / rb);
-    if (nraw > kGtRawMax) nraw = kGtRawMax;
-    if (nraw < 3) return HFB_ERR_UNSUPPORTED_GRID;
-    const size_t smem = 1024 + (size_t)nraw * rb + kGtOpStages * ob;
-    allow_max_dynamic_smem(gram_tma_kernel);
-    gram_tma_kernel<<<ncta, kGtThreads, smem, st>>>(job, maps, part, c->dev_status, c->wait_limit, nraw);
-  } else {
-    const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)npmax * 128);
-    allow_max_dynamic_smem(gram_tc_kernel);
-    gram_tc_kernel<<<ncta, kTcThreads, smem, st>>>(job, (const float*)psi, (const float*)hampsi,
-                                                   (const float*)hmfpsi, part, c->dev_status);
-  }
+  const size_t smem = 1024 + (size_t)kTcStages * (2 * kTcABytes + 2 * (size_t)npmax * 128);
+  allow_max_dynamic_smem(gram_tc_kernel);
+  gram_tc_kernel<<<ncta, kTcThreads, smem, st>>>(job, (const float*)psi, (const float*)hampsi,
+                                                 (const float*)hmfpsi, part, c->dev_status);
   HFB_CHECK_LAUNCH();
   TcOut ot;
   for (int q = 0; q < 8; ++q) ot.p[q] = outs_host[q];

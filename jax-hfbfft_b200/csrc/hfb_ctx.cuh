@@ -30,8 +30,6 @@ struct hfb_ctx_s {
   int f64_mma;           // FP64 Gram and rotation on the FP64 tensor cores (default; HFB_F64_MMA=0: CUDA cores)
   int tma_feed;          // single-precision rotation: K blocks by TMA, A in TMEM (default; HFB_TMA_FEED=0 at
                          // creation: producers that load through registers)
-  int gram_tma;          // single-precision Gram by the TMA-fed kernel (HFB_GRAM_TMA=1 at creation; measured
-                         // slower than the register-loaded producers, the default)
   long long wait_limit;  // clock cycles any one bounded device wait may take (hfb_set_wait_limit)
   int timeout_probe;     // the next tensor-core hpsi launch runs its timeout path (hfb_arm_timeout_probe)
   // scratch arena: fixed slots, grown on demand (never shrunk)

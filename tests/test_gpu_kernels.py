@@ -377,21 +377,6 @@ def test_gram_tensor_cores_match_cuda_cores(monkeypatch):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,s0,ns", [(16, 0, 140), (16, 5, 96), (24, 3, 9)])
-def test_gram_tma_matches_register_producers(monkeypatch, n, s0, ns):
-    """The TMA-fed Gram (A in tensor memory; HFB_GRAM_TMA=1 at context
-    creation) and the register-loaded one (the default) compute the same
-    three-term products: equal to within the fp32 accumulation order."""
-    g, a, vp = _gram_case(n, s0, ns, 13)
-    reg = _gram_run(g, a, vp, s0, ns, torch.complex64)
-    monkeypatch.setenv("HFB_GRAM_TMA", "1")
-    g2, _, _ = _gram_case(n, s0, ns, 13)
-    tma = _gram_run(g2, a, vp, s0, ns, torch.complex64)
-    for k in range(4):
-        assert rel(tma[k], reg[k]) < 1e-6, (k, rel(tma[k], reg[k]))
-
-
-@pytest.mark.gpu
 def test_diagstep_single_precision_matches_double():
     """hfb_diagstep on complex64 states (tensor-core Gram, Newton-Schulz
     S^-1/2, register-tiled rotation) against the same step on the complex128
@@ -433,13 +418,13 @@ def test_diagstep_single_precision_matches_double():
 
 
 @pytest.mark.gpu
-def test_diagstep_tma_feed_matches_register_producers(monkeypatch):
-    """One single-precision diagstep on Pb208 states (three 128-row Gram
-    blocks for the neutrons, rotation tasks over 48^3 x 2 grid points) with
-    the TMA-fed kernels (HFB_GRAM_TMA=1 for the Gram; the rotation's
-    default) and with the register-loaded producers of both (HFB_TMA_FEED=0,
-    the Gram's default): the same three-term products, so the rotated states
-    and the single-particle energies agree to single-precision rounding."""
+def test_rotation_tma_feed_matches_register_producers(monkeypatch):
+    """One single-precision diagstep on Pb208 states (rotation tasks over
+    48^3 x 2 grid points, three 72-output chunks for the neutrons) with the
+    TMA-fed rotation (the default) and with its register-loaded producers
+    (HFB_TMA_FEED=0 at context creation): the same three-term products, so
+    the rotated states and the single-particle energies agree to
+    single-precision rounding."""
     from hfb import config, static
 
     def run():
@@ -454,9 +439,7 @@ def test_diagstep_tma_feed_matches_register_producers(monkeypatch):
         st["grids"].ctx.check("diagstep")
         return st["levels"].psi.detach().clone(), st["levels"].sp_energy.detach().cpu().numpy().copy()
 
-    monkeypatch.setenv("HFB_GRAM_TMA", "1")
     p1, e1 = run()
-    monkeypatch.delenv("HFB_GRAM_TMA")
     monkeypatch.setenv("HFB_TMA_FEED", "0")
     p2, e2 = run()
     assert float((p1 - p2).abs().max()) <= 1e-4 * float(p2.abs().max())
