@@ -5,9 +5,10 @@
 // The complex product is written as one real GEMM over the interleaved
 // (re, im) storage: with A' = [Psi ; Psi~] (Psi~ row = (-im, re) per
 // element), D = A' X^T gives Re C in rows 0..n-1 and Im C in rows n..2n-1.
-// Operands are split as x = hi + lo with hi = tf32(x), lo = tf32(x - hi)
-// and D accumulates hi*hi + hi*lo + lo*hi (the three-term tf32 scheme,
-// about 22 significant bits per product).
+// Operands are split as x = hi + lo with hi = tf32(x), lo = x - hi (exact,
+// left unrounded: the MMA takes its tf32 part) and D accumulates hi*hi +
+// hi*lo + lo*hi (the three-term tf32 scheme, about 21 significant bits per
+// product).
 //
 // One CTA owns one 128-row block of A' for one matrix and one slice of K.
 // (Feeding the K blocks by TMA, with A split into tensor memory as the
@@ -167,10 +168,10 @@ gram_tc_kernel(TcJob job, const float* __restrict__ psi, const float* __restrict
       unsigned char* st = smem + (size_t)s * sbytes;
       auto put = [&](unsigned char* hi_base, uint32_t lo_delta, int row, float4 v) {
         float4 h, l;
-        h.x = tc::to_tf32(v.x); l.x = tc::to_tf32(v.x - h.x);
-        h.y = tc::to_tf32(v.y); l.y = tc::to_tf32(v.y - h.y);
-        h.z = tc::to_tf32(v.z); l.z = tc::to_tf32(v.z - h.z);
-        h.w = tc::to_tf32(v.w); l.w = tc::to_tf32(v.w - h.w);
+        tc::split_tf32(v.x, h.x, l.x);
+        tc::split_tf32(v.y, h.y, l.y);
+        tc::split_tf32(v.z, h.z, l.z);
+        tc::split_tf32(v.w, h.w, l.w);
         const uint32_t o = tc::sw128_offset(row, c);
         *reinterpret_cast<float4*>(hi_base + o) = h;
         *reinterpret_cast<float4*>(hi_base + lo_delta + o) = l;

@@ -89,10 +89,10 @@ __global__ void rot_b_prep_kernel(const double2* __restrict__ U, const double2* 
     v[q] = (float)x;
   }
   float4 h, l;
-  h.x = tc::to_tf32(v[0]); l.x = tc::to_tf32(v[0] - h.x);
-  h.y = tc::to_tf32(v[1]); l.y = tc::to_tf32(v[1] - h.y);
-  h.z = tc::to_tf32(v[2]); l.z = tc::to_tf32(v[2] - h.z);
-  h.w = tc::to_tf32(v[3]); l.w = tc::to_tf32(v[3] - h.w);
+  tc::split_tf32(v[0], h.x, l.x);
+  tc::split_tf32(v[1], h.y, l.y);
+  tc::split_tf32(v[2], h.z, l.z);
+  tc::split_tf32(v[3], h.w, l.w);
   unsigned char* base = bt + ((size_t)ch * nkb + kb) * 2 * kRtBBytes;
   const uint32_t o = tc::sw128_offset(row, c16);
   *reinterpret_cast<float4*>(base + o) = h;
@@ -184,10 +184,10 @@ rotate_tc_kernel(RtJob job, const float* __restrict__ psiT, const unsigned char*
         if (rl >= 128) continue;
         const float4 v = va[i];
         float4 h, l;
-        h.x = tc::to_tf32(v.x); l.x = tc::to_tf32(v.x - h.x);
-        h.y = tc::to_tf32(v.y); l.y = tc::to_tf32(v.y - h.y);
-        h.z = tc::to_tf32(v.z); l.z = tc::to_tf32(v.z - h.z);
-        h.w = tc::to_tf32(v.w); l.w = tc::to_tf32(v.w - h.w);
+        tc::split_tf32(v.x, h.x, l.x);
+        tc::split_tf32(v.y, h.y, l.y);
+        tc::split_tf32(v.z, h.z, l.z);
+        tc::split_tf32(v.w, h.w, l.w);
         const uint32_t o = tc::sw128_offset(rl, c);
         *reinterpret_cast<float4*>(st + o) = h;
         *reinterpret_cast<float4*>(st + kRtABytes + o) = l;
@@ -404,8 +404,7 @@ rotate_tma_kernel(RtJob job, const __grid_constant__ CUtensorMap mpt, const unsi
           const float x4[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            hv[4 * c4 + i] = tc::to_tf32(x4[i]);
-            lv[4 * c4 + i] = tc::to_tf32(x4[i] - hv[4 * c4 + i]);
+            tc::split_tf32(x4[i], hv[4 * c4 + i], lv[4 * c4 + i]);
           }
         }
         tc::tmem_st16(ta + 16 * half, hv);

@@ -237,5 +237,14 @@ __device__ __forceinline__ float to_tf32(float x) {
   return __uint_as_float(r);
 }
 
+// Three-term split x = hi + lo: hi = tf32(x) and lo = x - hi, exact in
+// fp32 and handed to the MMA without rounding (the MMA takes the tf32 part
+// of its 32-bit operands; what it drops of lo is below 2^-21 |x|, beside
+// the 2^-22 |x| of a rounded lo)
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+  hi = to_tf32(x);
+  lo = x - hi;
+}
+
 }  // namespace tc
 }  // namespace hfb
