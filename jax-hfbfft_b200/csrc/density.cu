@@ -27,6 +27,7 @@ struct DensGeo {
   static constexpr int THREADS = L * P;
   static constexpr int NB = N + 4;
   static constexpr int NTILE = (N * N + L - 1) / L;
+  static constexpr int WARPS = THREADS / 32;
 };
 
 // number of accumulated fields per axis kernel
@@ -46,7 +47,6 @@ density_axis_kernel(const cplx<R>* __restrict__ psi, int nst, int nneut, int nch
   constexpr size_t N2 = (size_t)N * N, N3 = N2 * N;
   __shared__ __align__(16) cplx<R> xball[G::L * G::NB];
   __shared__ cplx<R> tw[N];
-  __shared__ double kred[G::THREADS / 32];
   fill_twiddles<R>(tw, N);
   __syncthreads();
   const int tile = blockIdx.x;
@@ -71,15 +71,33 @@ density_axis_kernel(const cplx<R>* __restrict__ psi, int nst, int nneut, int nch
 #pragma unroll
     for (int m = 0; m < M; ++m) acc[f][m] = 0.0;
 
+  // the line values of the next state are loaded while this one is
+  // transformed and accumulated
+  Z an[M], bn[M];
+  if (sa < sb) {
+    const Z* ps = psi + (size_t)sa * 2 * N3 + base;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      an[m] = ps[(size_t)(p + P * m) * stride];
+      bn[m] = ps[N3 + (size_t)(p + P * m) * stride];
+    }
+  }
   for (int s = sa; s < sb; ++s) {
     const double w = want_fields ? wocc[s] * wstates[s] : 0.0;
     const double wu = want_fields ? wguv[s] * pairwg[s] * wstates[s] : 0.0;
-    const Z* ps = psi + (size_t)s * 2 * N3 + base;
     Z a[M], b[M], da[M], db[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-      a[m] = ps[(size_t)(p + P * m) * stride];
-      b[m] = ps[N3 + (size_t)(p + P * m) * stride];
+      a[m] = an[m];
+      b[m] = bn[m];
+    }
+    if (s + 1 < sb) {
+      const Z* ps = psi + (size_t)(s + 1) * 2 * N3 + base;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        an[m] = ps[(size_t)(p + P * m) * stride];
+        bn[m] = ps[N3 + (size_t)(p + P * m) * stride];
+      }
     }
     double knyq = 0.0;
     // D_d psi for both components (cderv d00: k = 0 and Nyquist zeroed)
@@ -143,16 +161,13 @@ density_axis_kernel(const cplx<R>* __restrict__ psi, int nst, int nneut, int nch
     }
     kin += nyq_fac * knyq;
     if (!active) kin = 0.0;
+    if (kin_part) {
+      // per-warp partials, summed in a fixed order by kinetic_reduce_kernel
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) kin += __shfl_xor_sync(0xffffffffu, kin, o);
-    if ((threadIdx.x & 31) == 0) kred[threadIdx.x / 32] = kin;
-    __syncthreads();
-    if (threadIdx.x == 0 && kin_part) {
-      double t = 0;
-      for (int i = 0; i < G::THREADS / 32; ++i) t += kred[i];
-      kin_part[(size_t)s * G::NTILE + tile] = t;
+      for (int o = 16; o > 0; o >>= 1) kin += __shfl_xor_sync(0xffffffffu, kin, o);
+      if ((threadIdx.x & 31) == 0)
+        kin_part[((size_t)s * G::NTILE + tile) * G::WARPS + threadIdx.x / 32] = kin;
     }
-    __syncthreads();
   }
   if (want_fields && active) {
     double* dst = part + (size_t)blockIdx.y * NF * N3;
@@ -204,15 +219,16 @@ __global__ void density_combine_kernel(size_t n3, int nchunk, const double* pz, 
   so[v + 2 * n3] = fx[3] + fy[3];
 }
 
-// sp_kinetic[s] = wxyz h2m_q sum over axes and tiles.
-__global__ void kinetic_reduce_kernel(int nst, int nneut, int ntile, const double* kz, const double* ky,
+// sp_kinetic[s] = wxyz h2m_q sum over axes, tiles and warps (``np`` partials
+// per state and axis).
+__global__ void kinetic_reduce_kernel(int nst, int nneut, int np, const double* kz, const double* ky,
                                       const double* kx, double wxyz, double h2m_n, double h2m_p, double* out) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nst) return;
   double t = 0;
-  for (int j = 0; j < ntile; ++j) t += kx[(size_t)s * ntile + j];
-  for (int j = 0; j < ntile; ++j) t += ky[(size_t)s * ntile + j];
-  for (int j = 0; j < ntile; ++j) t += kz[(size_t)s * ntile + j];
+  for (int j = 0; j < np; ++j) t += kx[(size_t)s * np + j];
+  for (int j = 0; j < np; ++j) t += ky[(size_t)s * np + j];
+  for (int j = 0; j < np; ++j) t += kz[(size_t)s * np + j];
   out[s] = wxyz * (s >= nneut ? h2m_p : h2m_n) * t;
 }
 
@@ -236,15 +252,15 @@ int density_launch_t(hfb_ctx_s* c, int nst, int nneut, const void* psi, const do
   }
   double* kin = nullptr;
   if (sp_kinetic) {
-    kin = (double*)scratch(c, hfb_ctx_s::S_RED, sizeof(double) * (size_t)3 * nst * G::NTILE);
+    kin = (double*)scratch(c, hfb_ctx_s::S_RED, sizeof(double) * (size_t)3 * nst * G::NTILE * G::WARPS);
     if (!kin) return HFB_ERR_ALLOC;
   }
   double* pz = part;
   double* py = part ? part + (size_t)nb * 9 * N3 : nullptr;
   double* px = part ? py + (size_t)nb * 4 * N3 : nullptr;
   double* kz = kin;
-  double* ky = kin ? kin + (size_t)nst * G::NTILE : nullptr;
-  double* kx = kin ? kin + (size_t)2 * nst * G::NTILE : nullptr;
+  double* ky = kin ? kin + (size_t)nst * G::NTILE * G::WARPS : nullptr;
+  double* kx = kin ? kin + (size_t)2 * nst * G::NTILE * G::WARPS : nullptr;
   dim3 grid(G::NTILE, nb);
   const double ks[3] = {2.0 * kPi / (c->d[0] * N) / N, 2.0 * kPi / (c->d[1] * N) / N, 2.0 * kPi / (c->d[2] * N) / N};
   double nf[3];
@@ -264,8 +280,8 @@ int density_launch_t(hfb_ctx_s* c, int nst, int nneut, const void* psi, const do
     HFB_CHECK_LAUNCH();
   }
   if (sp_kinetic) {
-    kinetic_reduce_kernel<<<(nst + 127) / 128, 128, 0, st>>>(nst, nneut, G::NTILE, kz, ky, kx, c->wxyz, h2m[0],
-                                                            h2m[1], sp_kinetic);
+    kinetic_reduce_kernel<<<(nst + 127) / 128, 128, 0, st>>>(nst, nneut, G::NTILE * G::WARPS, kz, ky, kx, c->wxyz,
+                                                            h2m[0], h2m[1], sp_kinetic);
     HFB_CHECK_LAUNCH();
   }
   return HFB_OK;
