@@ -100,7 +100,9 @@ precond_a_kernel(const cplx<R>* __restrict__ src, const cplx<R>* __restrict__ la
   const size_t off = (size_t)s * 2 * N3 + (size_t)x0 * N2;
   const R cf = coef ? (R)coef[s] : R(0);
   double n1 = 0, n2 = 0;
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
+  // compile-time trip count, unrolled: several loads in flight per thread
+#pragma unroll 8
+  for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
     int c = e / (N * N), r = e - c * N * N;
     size_t g = off + (size_t)c * N3 + r;
     Z v = src[g];
@@ -133,7 +135,9 @@ precond_a_kernel(const cplx<R>* __restrict__ src, const cplx<R>* __restrict__ la
   __syncthreads();
   for (int c = 0; c < 2; ++c) plane_lines<R, N, false, -1>(plane + c * N * G::LD, xb, tw, line, p, active);
   __syncthreads();
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
+  // compile-time trip count, unrolled: several loads in flight per thread
+#pragma unroll 8
+  for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
     int c = e / (N * N), r = e - c * N * N;
     tmp[off + (size_t)c * N3 + r] = plane[(c * N + r / N) * G::LD + r % N];
   }
@@ -158,7 +162,9 @@ precond_b_kernel(cplx<R>* tmp, int nneut, const double* __restrict__ wg, const d
   const int iq = s >= nneut ? 1 : 0;
   fill_twiddles<R>(tw, N);
   const size_t off = (size_t)s * 2 * N3 + (size_t)y0 * N;
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
+  // compile-time trip count, unrolled: several loads in flight per thread
+#pragma unroll 8
+  for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
     int c = e / (N * N), r = e - c * N * N;
     int a = r / N, b = r % N;
     plane[(c * N + a) * G::LD + b] = tmp[off + (size_t)c * N3 + (size_t)a * N2 + b];
@@ -198,7 +204,9 @@ precond_b_kernel(cplx<R>* tmp, int nneut, const double* __restrict__ wg, const d
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
+  // compile-time trip count, unrolled: several loads in flight per thread
+#pragma unroll 8
+  for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
     int c = e / (N * N), r = e - c * N * N;
     int a = r / N, b = r % N;
     tmp[off + (size_t)c * N3 + (size_t)a * N2 + b] = plane[(c * N + a) * G::LD + b];
@@ -219,7 +227,9 @@ precond_c_kernel(const cplx<R>* tmp, int mode, double x0, const double* x0_dev, 
   const int xp = blockIdx.x, s = blockIdx.y;
   fill_twiddles<R>(tw, N);
   const size_t off = (size_t)s * 2 * N3 + (size_t)xp * N2;
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
+  // compile-time trip count, unrolled: several loads in flight per thread
+#pragma unroll 8
+  for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
     int c = e / (N * N), r = e - c * N * N;
     plane[(c * N + r / N) * G::LD + r % N] = tmp[off + (size_t)c * N3 + r];
   }
@@ -233,7 +243,9 @@ precond_c_kernel(const cplx<R>* tmp, int mode, double x0, const double* x0_dev, 
   for (int c = 0; c < 2; ++c) plane_lines<R, N, true, +1>(plane + c * N * G::LD, xb, tw, line, p, active);
   __syncthreads();
   const R xr = (R)(x0_dev ? *x0_dev : x0);
-  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
+  // compile-time trip count, unrolled: several loads in flight per thread
+#pragma unroll 8
+  for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
     int c = e / (N * N), r = e - c * N * N;
     size_t g = off + (size_t)c * N3 + r;
     Z v = plane[(c * N + r / N) * G::LD + r % N];

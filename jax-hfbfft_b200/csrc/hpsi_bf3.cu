@@ -365,6 +365,14 @@ __device__ __forceinline__ void hb_tile(const HbArgs& a, const HbThread& t, HbSh
   tc::tmem_st_wait();
   tc::fence_before();
   __syncthreads();
+  // The pointwise step's first global inputs do not depend on GEMM 1:
+  // they are loaded while it runs.
+  const float4* fp = a.F + ((size_t)iq * 3 + AX) * N3 + hb_fidx<N>(L, t.j0);
+  float4 fn[4];
+  float2 pn[4];
+  hb_load_chunk<N, AX>(a.psi, cb, 0, pn);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) fn[i] = __ldg(fp + i * kHbLines);
   // ---- GEMM 1: e = D psi
   if (threadIdx.x == 0) {
     tc::fence_after();
@@ -389,12 +397,6 @@ __device__ __forceinline__ void hb_tile(const HbArgs& a, const HbThread& t, HbSh
   // The global loads of chunk k + 1 are issued before the TMEM accesses of
   // chunk k (which the compiler cannot reorder memory operations across),
   // so they are in flight while chunk k is computed.
-  const float4* fp = a.F + ((size_t)iq * 3 + AX) * N3 + hb_fidx<N>(L, t.j0);
-  float4 fn[4];
-  float2 pn[4];
-  hb_load_chunk<N, AX>(a.psi, cb, 0, pn);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) fn[i] = __ldg(fp + i * kHbLines);
 #pragma unroll
   for (int k = 0; k < G::NCK; ++k) {
     float4 f[4];
