@@ -100,8 +100,6 @@ precond_a_kernel(const cplx<R>* __restrict__ src, const cplx<R>* __restrict__ la
   const size_t off = (size_t)s * 2 * N3 + (size_t)x0 * N2;
   const R cf = coef ? (R)coef[s] : R(0);
   double n1 = 0, n2 = 0;
-  // compile-time trip count, unrolled: several loads in flight per thread
-#pragma unroll 8
   for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
     int c = e / (N * N), r = e - c * N * N;
     size_t g = off + (size_t)c * N3 + r;
@@ -135,8 +133,6 @@ precond_a_kernel(const cplx<R>* __restrict__ src, const cplx<R>* __restrict__ la
   __syncthreads();
   for (int c = 0; c < 2; ++c) plane_lines<R, N, false, -1>(plane + c * N * G::LD, xb, tw, line, p, active);
   __syncthreads();
-  // compile-time trip count, unrolled: several loads in flight per thread
-#pragma unroll 8
   for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
     int c = e / (N * N), r = e - c * N * N;
     tmp[off + (size_t)c * N3 + r] = plane[(c * N + r / N) * G::LD + r % N];
