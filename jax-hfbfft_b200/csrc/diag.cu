@@ -1762,7 +1762,7 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
     // Jacobi sweeps); FP32: the looser Jacobi threshold converges in a few
     // sweeps, hidden behind the Newton-Schulz GEMMs, and measured faster
     // than the refinement's longer launch sequence
-    if (ctx->lambda_refine && prec == HFB_F64) {
+    if (ctx->lambda_refine && (prec == HFB_F64 || ctx->lambda_refine_f32)) {
       r = eigh_refine(ctx, 2, nper, ld, gm + sm, 4 * sm, w + 2 * ld, ld, Vl, sm, tol_rel, es);
     } else {
       EighBatch eb{};
