@@ -124,8 +124,6 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     c->use_tcgen05 = (e && e[0] == '1') ? 0 : 1;
     const char* j = getenv("HFB_LAMBDA_JACOBI");
     c->lambda_refine = (j && j[0] == '1') ? 0 : 1;
-    const char* jf = getenv("HFB_LAMBDA_F32");
-    c->lambda_refine_f32 = (jf && strcmp(jf, "refine") == 0) ? 1 : 0;
     // single-precision hpsi kernel: bf16x3 (default), tf32x3 or fft (HFB_HPSI_KERNEL)
     const char* h = getenv("HFB_HPSI_KERNEL");
     c->hpsi_kind = (h && strcmp(h, "tf32x3") == 0) ? 1 : (h && strcmp(h, "fft") == 0) ? 2 : 0;

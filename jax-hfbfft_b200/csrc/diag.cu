@@ -472,6 +472,31 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
   for (; sweep < kJacMaxSweeps; ++sweep) {
     if (threadIdx.x == 0) any_rot = 0;
     __syncthreads();
+    // a sweep in which every pair is negligible at its start rotates nothing
+    // (the matrix never changes), so it is skipped after one parallel check
+    // of all pairs instead of being run round by round
+    {
+      int need = 0;
+      for (int e = threadIdx.x; e < m * (m - 1) / 2 && !need; e += blockDim.x) {
+        int k = (int)((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
+        while (k * (k + 1) / 2 > e) --k;
+        while ((k + 1) * (k + 2) / 2 <= e) ++k;
+        const int p_ = k + 1, q_ = e - k * (k + 1) / 2;   // p_ > q_
+        const double app = a[pk(p_, p_)].x, aqq = a[pk(q_, q_)].x;
+        const double2 apq = ld_h(a, p_, q_);
+        const double mag = hypot(apq.x, apq.y);
+        const bool negl = (mag <= tol_abs) ||
+                          (fabs(app) + 100.0 * mag == fabs(app) && fabs(aqq) + 100.0 * mag == fabs(aqq));
+        if (!negl) need = 1;
+      }
+      if (need) any_rot = 1;
+      __syncthreads();
+      const int go = any_rot;
+      __syncthreads();
+      if (!go) break;
+      if (threadIdx.x == 0) any_rot = 0;
+      __syncthreads();
+    }
     for (int r = 0; r < m - 1; ++r) {
       for (int q = threadIdx.x; q < half; q += blockDim.x) {
         int p_, q_;
@@ -1759,10 +1784,11 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
     // lambda; converging below that level refines nothing
     const double tol_rel = prec != HFB_F64 ? 5.9604644775390625e-08 : 0.0;
     // FP64: refinement (measured 1 ms per Pb208 iteration faster than the
-    // Jacobi sweeps); FP32: the looser Jacobi threshold converges in a few
-    // sweeps, hidden behind the Newton-Schulz GEMMs, and measured faster
-    // than the refinement's longer launch sequence
-    if (ctx->lambda_refine && (prec == HFB_F64 || ctx->lambda_refine_f32)) {
+    // Jacobi sweeps near convergence); FP32: the looser Jacobi threshold
+    // converges in a few sweeps and measured faster (11.4 ms against 12.0
+    // ms per Pb208 iteration: in the bulk the refinement's acceptance test
+    // fails and the Jacobi runs after it)
+    if (ctx->lambda_refine && prec == HFB_F64) {
       r = eigh_refine(ctx, 2, nper, ld, gm + sm, 4 * sm, w + 2 * ld, ld, Vl, sm, tol_rel, es);
     } else {
       EighBatch eb{};

@@ -22,8 +22,6 @@ struct hfb_ctx_s {
                          // HFB_NO_TCGEN05=1 in the environment at creation selects CUDA cores)
   int lambda_refine;     // FP64 diagstep diagonalises lambda by eigen refinement (default 1;
                          // HFB_LAMBDA_JACOBI=1 at creation selects the Jacobi solver)
-  int lambda_refine_f32; // the same for the single-precision diagstep (HFB_LAMBDA_F32=refine at creation;
-                         // default: Jacobi)
   cudaEvent_t ev_fork, ev_join;
   unsigned char* hpsi_b; // single-precision hpsi (tf32 kernel): derivative matrices in the tensor-core tile layout
   unsigned char* hpsi_bf3_b; // single-precision hpsi (bf16 three-term kernel): the same, bf16 h/m/l tiles
