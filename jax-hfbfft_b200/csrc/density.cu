@@ -220,16 +220,18 @@ __global__ void density_combine_kernel(size_t n3, int nchunk, const double* pz, 
 }
 
 // sp_kinetic[s] = wxyz h2m_q sum over axes, tiles and warps (``np`` partials
-// per state and axis).
+// per state and axis); one warp per state, lanes over strided partials, then
+// a fixed shuffle tree.
 __global__ void kinetic_reduce_kernel(int nst, int nneut, int np, const double* kz, const double* ky,
                                       const double* kx, double wxyz, double h2m_n, double h2m_p, double* out) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.x, lane = threadIdx.x;
   if (s >= nst) return;
   double t = 0;
-  for (int j = 0; j < np; ++j) t += kx[(size_t)s * np + j];
-  for (int j = 0; j < np; ++j) t += ky[(size_t)s * np + j];
-  for (int j = 0; j < np; ++j) t += kz[(size_t)s * np + j];
-  out[s] = wxyz * (s >= nneut ? h2m_p : h2m_n) * t;
+  for (int j = lane; j < np; j += 32)
+    t += kx[(size_t)s * np + j] + ky[(size_t)s * np + j] + kz[(size_t)s * np + j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (lane == 0) out[s] = wxyz * (s >= nneut ? h2m_p : h2m_n) * t;
 }
 
 template <class R, int N>
@@ -280,8 +282,8 @@ int density_launch_t(hfb_ctx_s* c, int nst, int nneut, const void* psi, const do
     HFB_CHECK_LAUNCH();
   }
   if (sp_kinetic) {
-    kinetic_reduce_kernel<<<(nst + 127) / 128, 128, 0, st>>>(nst, nneut, G::NTILE * G::WARPS, kz, ky, kx, c->wxyz,
-                                                            h2m[0], h2m[1], sp_kinetic);
+    kinetic_reduce_kernel<<<nst, 32, 0, st>>>(nst, nneut, G::NTILE * G::WARPS, kz, ky, kx, c->wxyz, h2m[0], h2m[1],
+                                              sp_kinetic);
     HFB_CHECK_LAUNCH();
   }
   return HFB_OK;

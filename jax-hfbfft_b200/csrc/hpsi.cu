@@ -182,9 +182,7 @@ hpsi_xplane_kernel(const R* __restrict__ pot, const cplx<R>* __restrict__ psi, c
   const R* potq = pot + (size_t)iq * 12 * N3;
   fill_twiddles<R>(tw, N);
   const Z* src = psi + (size_t)s * 2 * N3 + (size_t)x0 * N2;
-  // compile-time trip count, unrolled: several loads in flight per thread
-#pragma unroll 8
-  for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
+  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
     int c = e / (N * N), r = e - c * N * N;
     plane[(c * N + r / N) * G::LD + r % N] = src[(size_t)c * N3 + r];
   }
@@ -243,9 +241,7 @@ hpsi_yplane_kernel(const R* __restrict__ pot, const cplx<R>* __restrict__ psi, c
   fill_twiddles<R>(tw, N);
   const Z* src = psi + (size_t)s * 2 * N3 + (size_t)y0 * N;
   // plane (a = x, b = z) at fixed y0
-  // compile-time trip count, unrolled: several loads in flight per thread
-#pragma unroll 8
-  for (int e = threadIdx.x; e < 2 * N * N; e += G::THREADS) {
+  for (int e = threadIdx.x; e < 2 * N * N; e += blockDim.x) {
     int c = e / (N * N), r = e - c * N * N;
     int a = r / N, b = r % N;
     plane[(c * N + a) * G::LD + b] = src[(size_t)c * N3 + (size_t)a * N2 + b];
