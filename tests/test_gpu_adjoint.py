@@ -1,7 +1,7 @@
 """Sensitivities (hfb.adjoint) against central finite differences (relative
 step 1e-4) of the self-consistent solution, on the Ca48 sensitivity
 workload (32^3, dx 0.8 fm, 40 + 30 states, SLy4 + volume delta pairing):
-the binding energy's explicit gradient for all eleven Skyrme couplings and
+the binding energy's explicit gradient for the ten Skyrme couplings and
 both pairing strengths, and the proton rms radius's gradient by the
 implicit adjoint (linear-response solve at the fixed point).  Ca48 is
 doubly magic: its BCS gap all but collapses, the occupations are within
