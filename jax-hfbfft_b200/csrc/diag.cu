@@ -407,6 +407,7 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
   int* rq = rp + half;
   int* act = rq + half;
   __shared__ int any_rot;
+  __shared__ int round_rot[2];   // a rotation in round r (parity r & 1)
   const double2* Ab = eb.a[b];
   JacRot* rotb = rot + (size_t)b * rot_stride;
   // the lower triangle (eigh with symmetrize_input=False reads only it; the
@@ -497,7 +498,12 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
       if (threadIdx.x == 0) any_rot = 0;
       __syncthreads();
     }
+    if (threadIdx.x == 0) round_rot[0] = round_rot[1] = 0;
+    __syncthreads();
     for (int r = 0; r < m - 1; ++r) {
+      // the next round's flag is cleared here; no thread reads it before
+      // this round's barrier
+      if (threadIdx.x == 0) round_rot[(r + 1) & 1] = 0;
       for (int q = threadIdx.x; q < half; q += blockDim.x) {
         int p_, q_;
         rr_pair(m, r, q, p_, q_);
@@ -519,6 +525,7 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
           g.om = make_double2(apq.x / mag, -apq.y / mag);
           on = 1;
           any_rot = 1;
+          round_rot[r & 1] = 1;
         }
         rr[q] = g;
         rp[q] = p_;
@@ -527,6 +534,13 @@ jacobi_kernel(EighBatch eb, JacRot* rot, int* nrounds_out, int* status, size_t r
         rotb[(size_t)rounds * half + q] = g;
       }
       __syncthreads();
+      // a round without rotations leaves the matrix as it is: no update
+      // pass and no second barrier (the next round's first writes to the
+      // rotation arrays come after every thread has passed this test)
+      if (!round_rot[r & 1]) {
+        ++rounds;
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < kJacBlk; ++j) {
         const int q1 = bq1[j], q2 = bq2[j];
