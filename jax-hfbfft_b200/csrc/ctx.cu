@@ -46,6 +46,7 @@ bool encode_fp32_rows_map(CUtensorMap* m, const void* base, uint64_t row_floats,
 int coulomb_init(hfb_ctx_s* c);  // skyrme.cu
 int hpsi_tc_prepare(hfb_ctx_s* c);   // hpsi_tc.cu
 int hpsi_bf3_prepare(hfb_ctx_s* c);  // hpsi_bf3.cu
+int hpsi_dmma_prepare(hfb_ctx_s* c); // hpsi_dmma.cu
 
 void* scratch(hfb_ctx_s* c, int s, size_t bytes) {
   if (s < 0 || s >= hfb_ctx_s::S_NSLOT) return nullptr;
@@ -131,6 +132,8 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     const char* gk = getenv("HFB_F64_MMA");
     c->f64_mma = (gk && gk[0] == '0') ? 0 : 1;
     // single-precision rotation fed by TMA unless HFB_TMA_FEED=0
+    const char* fh = getenv("HFB_F64_HPSI");
+    c->f64_hpsi = (fh && strcmp(fh, "dmma") == 0) ? 1 : 0;
     const char* gt = getenv("HFB_TMA_FEED");
     c->tma_feed = (gt && gt[0] == '0') ? 0 : 1;
     c->wait_limit = kDefaultWaitLimit;
@@ -167,6 +170,7 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
   int r = coulomb_init(c);
   if (r == HFB_OK) r = hpsi_tc_prepare(c);
   if (r == HFB_OK) r = hpsi_bf3_prepare(c);
+  if (r == HFB_OK) r = hpsi_dmma_prepare(c);
   if (r == HFB_OK && cudaDeviceSynchronize() != cudaSuccess) r = HFB_ERR_CUDA;
   if (r != HFB_OK) {
     hfb_ctx_destroy(c);
@@ -186,6 +190,7 @@ extern "C" int hfb_ctx_destroy(hfb_ctx_t c) {
   if (c->coul_q) cudaFree(c->coul_q);
   if (c->hpsi_b) cudaFree(c->hpsi_b);
   if (c->hpsi_bf3_b) cudaFree(c->hpsi_bf3_b);
+  if (c->hpsi_d64) cudaFree(c->hpsi_d64);
   if (c->dev_status) cudaFree(c->dev_status);
   if (c->side) {
     cudaStreamDestroy(c->side);

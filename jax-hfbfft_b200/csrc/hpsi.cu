@@ -338,6 +338,8 @@ int hpsi_launch(hfb_ctx_s* c, int prec, const void* pot, int s0, int ns, int nne
     return hpsi_bf3_launch(c, pot, s0, ns, nneut, psi, weight, weightuv, acc, pout, pout_mf, pout_del, ovl, st);
   if (hpsi_tc_available(c, prec))
     return hpsi_tc_launch(c, pot, s0, ns, nneut, psi, weight, weightuv, acc, pout, pout_mf, pout_del, ovl, st);
+  if (hpsi_dmma_available(c, prec))
+    return hpsi_dmma_launch(c, pot, s0, ns, nneut, psi, weight, weightuv, acc, pout, pout_mf, pout_del, ovl, st);
   return dispatch_n(c->n, [&](auto nn) -> int {
     constexpr int N = decltype(nn)::value;
     if (prec == HFB_F64)

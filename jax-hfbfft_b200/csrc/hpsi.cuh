@@ -29,6 +29,15 @@ int hpsi_bf3_launch(hfb_ctx_s* c, const void* pot, int s0, int ns, int nneut, co
                     const double* weightuv, void* acc, void* pout, void* pout_mf, void* pout_del, double* ovl,
                     cudaStream_t st);
 
+// Double-precision hpsi on the FP64 tensor cores (hpsi_dmma.cu): the
+// derivative matrices in double, built at context creation; same contract
+// and overlap partials (one per y-plane) as the FFT kernels.
+int hpsi_dmma_prepare(hfb_ctx_s* c);
+bool hpsi_dmma_available(hfb_ctx_s* c, int prec);
+int hpsi_dmma_launch(hfb_ctx_s* c, const void* pot, int s0, int ns, int nneut, const void* psi, const double* weight,
+                     const double* weightuv, void* acc, void* pout, void* pout_mf, void* pout_del, double* ovl,
+                     cudaStream_t st);
+
 // Partial sums per state that hpsi_launch writes into ``ovl``.
 int hpsi_ovl_parts(hfb_ctx_s* c, int prec);
 

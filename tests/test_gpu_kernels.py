@@ -102,6 +102,19 @@ def test_hpsi_batched_against_oracle(n, dtype, ns):
     """Batched hpsi over states of both isospins on larger grids vs the oracle
     (single precision on 24-48 grids runs the tensor-core kernel; 37 states on
     24^3 span several scheduling groups, the last one partial)."""
+    _check_hpsi_batched(n, dtype, ns)
+
+
+@pytest.mark.parametrize("n,ns", [(8, 3), (16, 5), (24, 5), (40, 5), (48, 5), (48, 9)])
+def test_hpsi_fp64_tensor_cores_against_oracle(monkeypatch, n, ns):
+    """FP64 hpsi on the FP64 tensor cores (HFB_F64_HPSI=dmma at context
+    creation: D as an n x n matrix, mma.sync m8n8k4 .f64) against the oracle,
+    to the same 1e-11 as the FFT kernels."""
+    monkeypatch.setenv("HFB_F64_HPSI", "dmma")
+    _check_hpsi_batched(n, torch.complex128, ns)
+
+
+def _check_hpsi_batched(n, dtype, ns):
     import hfb
     from oracle import model, meanfield as omf
     rng = np.random.default_rng(n)
