@@ -71,13 +71,14 @@ constexpr int hd_dld() { return HdGeo<N>::DLD; }
 
 // One axis pass over the N lines of the staged plane X: emits the axis's
 // contribution to h x at every point of the plane, both spinor components,
-// through emit(line, j, g, out0, out1) (g the point's index in the state).
+// through emit(line, j, g, out0, out1, pre(g)) (g the point's index in the
+// state; pre's global loads are issued before the tile's GEMM 2 MMAs).
 // Dm is D for the axis (row stride hd_dld), W a second plane buffer, alt and
 // bbar per-line scratch; lines start at base + line * sa (ROW) or base +
 // line * sb, points are sb (ROW) or sa apart.  Ends with a CTA barrier.
-template <int N, int AXIS, bool ROW, bool LOCAL, class Emit>
+template <int N, int AXIS, bool ROW, bool LOCAL, class Pre, class Emit>
 __device__ __forceinline__ void hd_pass(const double2* X, double2* W, const double* Dm, double2* alt, double* bbar,
-                                        const double* pot, size_t base, size_t sa, size_t sb, double nq,
+                                        const double* pot, size_t base, size_t sa, size_t sb, double nq, Pre&& pre,
                                         Emit&& emit) {
   using G = HdGeo<N>;
   constexpr size_t N3 = (size_t)N * N * N;
@@ -87,21 +88,32 @@ __device__ __forceinline__ void hd_pass(const double2* X, double2* W, const doub
     return ROW ? base + (size_t)line * sa + (size_t)j * sb : base + (size_t)j * sa + (size_t)line * sb;
   };
   // Nyquist ingredients per line (levels.py:314-330): sum_l (-1)^l x_l of
-  // both components and the line mean of B
-  for (int i = tid; i < 2 * N; i += kHdThreads) {
-    const int c = i / N, line = i % N;
-    double sx = 0.0, sy = 0.0;
-    for (int l = 0; l < N; ++l) {
-      const double2 v = X[hd_at<N, ROW>(c, line, l)];
-      sx += (l & 1) ? -v.x : v.x;
-      sy += (l & 1) ? -v.y : v.y;
+  // both components and the line mean of B; one warp per line, lanes over
+  // the points, a fixed shuffle tree
+  for (int line = warp; line < N; line += kHdWarps) {
+    double ax0 = 0.0, ay0 = 0.0, ax1 = 0.0, ay1 = 0.0, bs = 0.0;
+    for (int l = lane; l < N; l += 32) {
+      const double sgn = (l & 1) ? -1.0 : 1.0;
+      const double2 v0 = X[hd_at<N, ROW>(0, line, l)], v1 = X[hd_at<N, ROW>(1, line, l)];
+      ax0 += sgn * v0.x;
+      ay0 += sgn * v0.y;
+      ax1 += sgn * v1.x;
+      ay1 += sgn * v1.y;
+      bs += pot[1 * N3 + gidx(line, l)];
     }
-    alt[i] = make_double2(sx, sy);
-  }
-  for (int line = tid; line < N; line += kHdThreads) {
-    double sb_ = 0.0;
-    for (int l = 0; l < N; ++l) sb_ += pot[1 * N3 + gidx(line, l)];
-    bbar[line] = sb_ / N;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ax0 += __shfl_xor_sync(0xffffffffu, ax0, o);
+      ay0 += __shfl_xor_sync(0xffffffffu, ay0, o);
+      ax1 += __shfl_xor_sync(0xffffffffu, ax1, o);
+      ay1 += __shfl_xor_sync(0xffffffffu, ay1, o);
+      bs += __shfl_xor_sync(0xffffffffu, bs, o);
+    }
+    if (lane == 0) {
+      alt[line] = make_double2(ax0, ay0);
+      alt[N + line] = make_double2(ax1, ay1);
+      bbar[line] = bs / N;
+    }
   }
   // MMA fragments: A = D rows j0 + lane/4, k = lane%4; B = the plane's line
   // l0 + lane/8, re (lane/4 even) or im, k = lane%4; C = point j0 + lane/4,
@@ -115,6 +127,20 @@ __device__ __forceinline__ void hd_pass(const double2* X, double2* W, const doub
     const int t = warp + ti * kHdWarps;
     if (t < G::NT) {
       const int j0 = (t / G::LG) * 8, l0 = (t % G::LG) * 4;
+      // this tile's pointwise inputs are loaded before its MMAs, which hide
+      // their latency
+      const int line = l0 + (lane & 3), j = j0 + (lane >> 2);
+      const size_t g = gidx(line, j);
+      const double bm = pot[1 * N3 + g];
+      const double aqd = pot[(3 + AXIS) * N3 + g];
+      const double w0 = pot[9 * N3 + g], w1 = pot[10 * N3 + g], w2 = pot[11 * N3 + g];
+      double up = 0.0, s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      if (LOCAL) {
+        up = pot[g];
+        s0 = pot[6 * N3 + g];
+        s1 = pot[7 * N3 + g];
+        s2 = pot[8 * N3 + g];
+      }
       double c0[2] = {0.0, 0.0}, c1[2] = {0.0, 0.0};
 #pragma unroll
       for (int ks = 0; ks < G::KS; ++ks) {
@@ -124,17 +150,11 @@ __device__ __forceinline__ void hd_pass(const double2* X, double2* W, const doub
         hd_mma(c0, a, bri ? x0.y : x0.x);
         hd_mma(c1, a, bri ? x1.y : x1.x);
       }
-      const int line = l0 + (lane & 3), j = j0 + (lane >> 2);
-      const size_t g = gidx(line, j);
       const double2 e0 = make_double2(c0[0], c0[1]), e1 = make_double2(c1[0], c1[1]);
       const double2 a0 = X[hd_at<N, ROW>(0, line, j)], a1 = X[hd_at<N, ROW>(1, line, j)];
-      const double bm = pot[1 * N3 + g];
-      const double aqd = pot[(3 + AXIS) * N3 + g];
-      const double w0 = pot[9 * N3 + g], w1 = pot[10 * N3 + g], w2 = pot[11 * N3 + g];
       double2 q0, q1, n0, n1;
       if (LOCAL) {
         // upot psi + sigma.spot psi (meanfield.py:47-58)
-        const double up = pot[g], s0 = pot[6 * N3 + g], s1 = pot[7 * N3 + g], s2 = pot[8 * N3 + g];
         q0 = (up + s2) * a0 + cmulri(s0, -s1, a1);
         q1 = (up - s2) * a1 + cmulri(s0, s1, a0);
       } else {
@@ -173,6 +193,9 @@ __device__ __forceinline__ void hd_pass(const double2* X, double2* W, const doub
     const int t = warp + ti * kHdWarps;
     if (t < G::NT) {
       const int j0 = (t / G::LG) * 8, l0 = (t % G::LG) * 4;
+      const int line = l0 + (lane & 3), j = j0 + (lane >> 2);
+      const size_t g = gidx(line, j);
+      const auto pv = pre(g);
       double c0[2] = {0.0, 0.0}, c1[2] = {0.0, 0.0};
 #pragma unroll
       for (int ks = 0; ks < G::KS; ++ks) {
@@ -182,11 +205,10 @@ __device__ __forceinline__ void hd_pass(const double2* X, double2* W, const doub
         hd_mma(c0, a, bri ? x0.y : x0.x);
         hd_mma(c1, a, bri ? x1.y : x1.x);
       }
-      const int line = l0 + (lane & 3), j = j0 + (lane >> 2);
       const double sg = ((j & 1) ? -nq : nq) * bbar[line];
       const double2 r0 = o0[ti] + make_double2(c0[0], c0[1]) + sg * alt[line];
       const double2 r1 = o1[ti] + make_double2(c1[0], c1[1]) + sg * alt[N + line];
-      emit(line, j, gidx(line, j), r0, r1);
+      emit(line, j, g, r0, r1, pv);
     }
   }
   __syncthreads();
@@ -199,8 +221,15 @@ namespace {
 template <int N>
 __device__ __forceinline__ void hd_load_d(double* dst, const double* src) {
   constexpr int DLD = hd_dld<N>();
+#pragma unroll 4
   for (int e = threadIdx.x; e < N * N; e += kHdThreads) dst[(e / N) * DLD + e % N] = src[e];
 }
+
+// Values an emit step reads from global memory, loaded before its MMAs.
+struct HdPre {
+  double2 m0, m1;   // the state's partial h psi, both components
+  double vp;        // v_pair
+};
 
 // A: one x-plane of one state; z lines with the local terms, then y lines.
 template <int N>
@@ -220,6 +249,7 @@ hpsi_dmma_x_kernel(const double* __restrict__ pot, const double2* __restrict__ p
   const int x0 = blockIdx.x, s = s0 + blockIdx.y;
   const double* potq = pot + (size_t)(s >= nneut ? 1 : 0) * 12 * N3;
   const double2* src = psi + (size_t)s * 2 * N3 + (size_t)x0 * N2;
+#pragma unroll 6
   for (int e = threadIdx.x; e < 2 * N * N; e += kHdThreads) {
     const int c = e / (N * N), r = e - c * N * N;
     plane[(c * N + r / N) * G::LD + r % N] = src[(size_t)c * N3 + r];
@@ -229,16 +259,19 @@ hpsi_dmma_x_kernel(const double* __restrict__ pot, const double2* __restrict__ p
   __syncthreads();
   double2* dst = acc + (size_t)s * 2 * N3;
   const size_t base = (size_t)x0 * N2;
-  hd_pass<N, 2, true, true>(plane, wb, dz, alt, bbar, potq, base, N, 1, nq_z,
-                            [&](int, int, size_t g, double2 q0, double2 q1) {
-                              dst[g] = q0;
-                              dst[N3 + g] = q1;
-                            });
-  hd_pass<N, 1, false, false>(plane, wb, dy, alt, bbar, potq, base, N, 1, nq_y,
-                              [&](int, int, size_t g, double2 q0, double2 q1) {
-                                dst[g] = dst[g] + q0;
-                                dst[N3 + g] = dst[N3 + g] + q1;
-                              });
+  hd_pass<N, 2, true, true>(
+      plane, wb, dz, alt, bbar, potq, base, N, 1, nq_z, [](size_t) { return 0; },
+      [&](int, int, size_t g, double2 q0, double2 q1, int) {
+        dst[g] = q0;
+        dst[N3 + g] = q1;
+      });
+  hd_pass<N, 1, false, false>(
+      plane, wb, dy, alt, bbar, potq, base, N, 1, nq_y,
+      [&](size_t g) { return HdPre{dst[g], dst[N3 + g], 0.0}; },
+      [&](int, int, size_t g, double2 q0, double2 q1, const HdPre& pv) {
+        dst[g] = pv.m0 + q0;
+        dst[N3 + g] = pv.m1 + q1;
+      });
 }
 
 // B: one y-plane of one state; x lines, then pout = weight * h psi -
@@ -263,6 +296,7 @@ hpsi_dmma_y_kernel(const double* __restrict__ pot, const double2* __restrict__ p
   const double* potq = pot + (size_t)(s >= nneut ? 1 : 0) * 12 * N3;
   const double2* src = psi + (size_t)s * 2 * N3 + (size_t)y0 * N;
   // plane (a = x, b = z) at fixed y0
+#pragma unroll 6
   for (int e = threadIdx.x; e < 2 * N * N; e += kHdThreads) {
     const int c = e / (N * N), r = e - c * N * N;
     const int a = r / N, b = r % N;
@@ -276,12 +310,13 @@ hpsi_dmma_y_kernel(const double* __restrict__ pot, const double2* __restrict__ p
   const size_t so = (size_t)s * 2 * N3;
   double ov_mf = 0.0, ov_po = 0.0;
   hd_pass<N, 0, false, false>(plane, wb, dx, alt, bbar, potq, (size_t)y0 * N, N2, 1, nq_x,
-                              [&](int line, int j, size_t g, double2 q0, double2 q1) {
-                                const double vp = potq[2 * N3 + g];
+                              [&](size_t g) { return HdPre{a_s[g], a_s[N3 + g], potq[2 * N3 + g]}; },
+                              [&](int line, int j, size_t g, double2 q0, double2 q1, const HdPre& pv) {
+                                const double vp = pv.vp;
 #pragma unroll
                                 for (int c = 0; c < 2; ++c) {
                                   const size_t gi = (size_t)c * N3 + g;
-                                  const double2 mf = a_s[gi] + (c == 0 ? q0 : q1);
+                                  const double2 mf = (c == 0 ? pv.m0 : pv.m1) + (c == 0 ? q0 : q1);
                                   const double2 ps = plane[hd_at<N, false>(c, line, j)];
                                   const double2 dl = vp * ps;
                                   const double2 po = wt * mf - wu * dl;
