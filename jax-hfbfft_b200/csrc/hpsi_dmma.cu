@@ -35,9 +35,9 @@ constexpr int kHdThreads = 32 * kHdWarps;
 
 template <int N>
 struct HdGeo {
-  static constexpr int LD = N + 2;                     // complex elements per staged row
+  static constexpr int LD = N + 4;                     // complex elements per staged row (rows half a bank set apart)
   static constexpr int MB = N / 8;                     // 8-point blocks of a line
-  static constexpr int LG = N / 4;                     // 4-line groups of a plane
+  static constexpr int LG = N / 8;                     // 8-line groups of a plane
   static constexpr int NT = MB * LG;                   // MMA tiles per pass
   static constexpr int TMAX = (NT + kHdWarps - 1) / kHdWarps;
   static constexpr int KS = N / 4;                     // k steps
@@ -115,75 +115,87 @@ __device__ __forceinline__ void hd_pass(const double2* X, double2* W, const doub
       bbar[line] = bs / N;
     }
   }
-  // MMA fragments: A = D rows j0 + lane/4, k = lane%4; B = the plane's line
-  // l0 + lane/8, re (lane/4 even) or im, k = lane%4; C = point j0 + lane/4,
-  // line l0 + lane%4, (re, im)
-  const int bl_off = lane >> 3, bri = (lane >> 2) & 1;
+  // Tile: 8 points x 8 lines.  MMA fragments: A = D row j0 + lane/4, k =
+  // lane%4; B = line l0 + lane/4 at point k, one MMA each for the re and im
+  // parts of the two spinor components (one double2 load gives both parts);
+  // C = point j0 + lane/4, lines l0 + 2 (lane%4) + {0, 1}.
   const double h = 0.5;
-  double2 o0[G::TMAX], o1[G::TMAX];
+  double2 o[G::TMAX][2][2];   // [tile][line of the pair][component]
   // ---- GEMM 1: e = D x, then o = L_d e (+ local terms), w = L_d x - B e
 #pragma unroll
   for (int ti = 0; ti < G::TMAX; ++ti) {
     const int t = warp + ti * kHdWarps;
     if (t < G::NT) {
-      const int j0 = (t / G::LG) * 8, l0 = (t % G::LG) * 4;
+      const int j0 = (t / G::LG) * 8, l0 = (t % G::LG) * 8;
+      const int j = j0 + (lane >> 2), lp = l0 + 2 * (lane & 3);
       // this tile's pointwise inputs are loaded before its MMAs, which hide
       // their latency
-      const int line = l0 + (lane & 3), j = j0 + (lane >> 2);
-      const size_t g = gidx(line, j);
-      const double bm = pot[1 * N3 + g];
-      const double aqd = pot[(3 + AXIS) * N3 + g];
-      const double w0 = pot[9 * N3 + g], w1 = pot[10 * N3 + g], w2 = pot[11 * N3 + g];
-      double up = 0.0, s0 = 0.0, s1 = 0.0, s2 = 0.0;
-      if (LOCAL) {
-        up = pot[g];
-        s0 = pot[6 * N3 + g];
-        s1 = pot[7 * N3 + g];
-        s2 = pot[8 * N3 + g];
+      double bm[2], aqd[2], w0[2], w1[2], w2[2], up[2], s0[2], s1[2], s2[2];
+      size_t g[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        g[u] = gidx(lp + u, j);
+        bm[u] = pot[1 * N3 + g[u]];
+        aqd[u] = pot[(3 + AXIS) * N3 + g[u]];
+        w0[u] = pot[9 * N3 + g[u]];
+        w1[u] = pot[10 * N3 + g[u]];
+        w2[u] = pot[11 * N3 + g[u]];
+        up[u] = LOCAL ? pot[g[u]] : 0.0;
+        s0[u] = LOCAL ? pot[6 * N3 + g[u]] : 0.0;
+        s1[u] = LOCAL ? pot[7 * N3 + g[u]] : 0.0;
+        s2[u] = LOCAL ? pot[8 * N3 + g[u]] : 0.0;
       }
-      double c0[2] = {0.0, 0.0}, c1[2] = {0.0, 0.0};
+      double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
       for (int ks = 0; ks < G::KS; ++ks) {
         const int pt = ks * 4 + (lane & 3);
         const double a = Dm[(j0 + (lane >> 2)) * DLD + pt];
-        const double2 x0 = X[hd_at<N, ROW>(0, l0 + bl_off, pt)], x1 = X[hd_at<N, ROW>(1, l0 + bl_off, pt)];
-        hd_mma(c0, a, bri ? x0.y : x0.x);
-        hd_mma(c1, a, bri ? x1.y : x1.x);
+        const double2 x0 = X[hd_at<N, ROW>(0, l0 + (lane >> 2), pt)];
+        const double2 x1 = X[hd_at<N, ROW>(1, l0 + (lane >> 2), pt)];
+        hd_mma(acc[0], a, x0.x);
+        hd_mma(acc[1], a, x0.y);
+        hd_mma(acc[2], a, x1.x);
+        hd_mma(acc[3], a, x1.y);
       }
-      const double2 e0 = make_double2(c0[0], c0[1]), e1 = make_double2(c1[0], c1[1]);
-      const double2 a0 = X[hd_at<N, ROW>(0, line, j)], a1 = X[hd_at<N, ROW>(1, line, j)];
-      double2 q0, q1, n0, n1;
-      if (LOCAL) {
-        // upot psi + sigma.spot psi (meanfield.py:47-58)
-        q0 = (up + s2) * a0 + cmulri(s0, -s1, a1);
-        q1 = (up - s2) * a1 + cmulri(s0, s1, a0);
-      } else {
-        q0 = make_double2(0.0, 0.0);
-        q1 = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int line = lp + u;
+        const double2 e0 = make_double2(acc[0][u], acc[1][u]), e1 = make_double2(acc[2][u], acc[3][u]);
+        const double2 a0 = X[hd_at<N, ROW>(0, line, j)], a1 = X[hd_at<N, ROW>(1, line, j)];
+        double2 q0, q1, n0, n1;
+        if (LOCAL) {
+          // upot psi + sigma.spot psi (meanfield.py:47-58)
+          q0 = (up[u] + s2[u]) * a0 + cmulri(s0[u], -s1[u], a1);
+          q1 = (up[u] - s2[u]) * a1 + cmulri(s0[u], s1[u], a0);
+        } else {
+          q0 = make_double2(0.0, 0.0);
+          q1 = make_double2(0.0, 0.0);
+        }
+        const double aq = aqd[u], v0 = w0[u], v1 = w1[u], v2 = w2[u];
+        if (AXIS == 0) {
+          // meanfield.py:63-83
+          q0 = q0 + cmulri(0.0, -(h * aq - h * v1), e0) - (h * v2) * e1;
+          q1 = q1 + cmulri(0.0, -(h * aq + h * v1), e1) + (h * v2) * e0;
+          n0 = cmulri(0.0, -h * (aq - v1), a0) - (h * v2) * a1;
+          n1 = cmulri(0.0, -h * (aq + v1), a1) + (h * v2) * a0;
+        } else if (AXIS == 1) {
+          // meanfield.py:92-112
+          q0 = q0 + cmulri(0.0, -(h * aq + h * v0), e0) + cmulri(0.0, h * v2, e1);
+          q1 = q1 + cmulri(0.0, -(h * aq - h * v0), e1) + cmulri(0.0, h * v2, e0);
+          n0 = cmulri(0.0, -h * (aq + v0), a0) + cmulri(0.0, h * v2, a1);
+          n1 = cmulri(0.0, -h * (aq - v0), a1) + cmulri(0.0, h * v2, a0);
+        } else {
+          // meanfield.py:121-141
+          q0 = q0 + cmulri(0.0, -(h * aq), e0) + cmulri(h * v0, -(h * v1), e1);
+          q1 = q1 + cmulri(0.0, -(h * aq), e1) + cmulri(-(h * v0), -(h * v1), e0);
+          n0 = cmulri(0.0, -h * aq, a0) + cmulri(h * v0, -(h * v1), a1);
+          n1 = cmulri(0.0, -h * aq, a1) + cmulri(-(h * v0), -(h * v1), a0);
+        }
+        o[ti][u][0] = q0;
+        o[ti][u][1] = q1;
+        W[hd_at<N, ROW>(0, line, j)] = n0 - bm[u] * e0;
+        W[hd_at<N, ROW>(1, line, j)] = n1 - bm[u] * e1;
       }
-      if (AXIS == 0) {
-        // meanfield.py:63-83
-        q0 = q0 + cmulri(0.0, -(h * aqd - h * w1), e0) - (h * w2) * e1;
-        q1 = q1 + cmulri(0.0, -(h * aqd + h * w1), e1) + (h * w2) * e0;
-        n0 = cmulri(0.0, -h * (aqd - w1), a0) - (h * w2) * a1;
-        n1 = cmulri(0.0, -h * (aqd + w1), a1) + (h * w2) * a0;
-      } else if (AXIS == 1) {
-        // meanfield.py:92-112
-        q0 = q0 + cmulri(0.0, -(h * aqd + h * w0), e0) + cmulri(0.0, h * w2, e1);
-        q1 = q1 + cmulri(0.0, -(h * aqd - h * w0), e1) + cmulri(0.0, h * w2, e0);
-        n0 = cmulri(0.0, -h * (aqd + w0), a0) + cmulri(0.0, h * w2, a1);
-        n1 = cmulri(0.0, -h * (aqd - w0), a1) + cmulri(0.0, h * w2, a0);
-      } else {
-        // meanfield.py:121-141
-        q0 = q0 + cmulri(0.0, -(h * aqd), e0) + cmulri(h * w0, -(h * w1), e1);
-        q1 = q1 + cmulri(0.0, -(h * aqd), e1) + cmulri(-(h * w0), -(h * w1), e0);
-        n0 = cmulri(0.0, -h * aqd, a0) + cmulri(h * w0, -(h * w1), a1);
-        n1 = cmulri(0.0, -h * aqd, a1) + cmulri(-(h * w0), -(h * w1), a0);
-      }
-      o0[ti] = q0;
-      o1[ti] = q1;
-      W[hd_at<N, ROW>(0, line, j)] = n0 - bm * e0;
-      W[hd_at<N, ROW>(1, line, j)] = n1 - bm * e1;
     }
   }
   __syncthreads();
@@ -192,23 +204,32 @@ __device__ __forceinline__ void hd_pass(const double2* X, double2* W, const doub
   for (int ti = 0; ti < G::TMAX; ++ti) {
     const int t = warp + ti * kHdWarps;
     if (t < G::NT) {
-      const int j0 = (t / G::LG) * 8, l0 = (t % G::LG) * 4;
-      const int line = l0 + (lane & 3), j = j0 + (lane >> 2);
-      const size_t g = gidx(line, j);
-      const auto pv = pre(g);
-      double c0[2] = {0.0, 0.0}, c1[2] = {0.0, 0.0};
+      const int j0 = (t / G::LG) * 8, l0 = (t % G::LG) * 8;
+      const int j = j0 + (lane >> 2), lp = l0 + 2 * (lane & 3);
+      const size_t g0 = gidx(lp, j), g1 = gidx(lp + 1, j);
+      const auto pv0 = pre(g0);
+      const auto pv1 = pre(g1);
+      double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
       for (int ks = 0; ks < G::KS; ++ks) {
         const int pt = ks * 4 + (lane & 3);
         const double a = Dm[(j0 + (lane >> 2)) * DLD + pt];
-        const double2 x0 = W[hd_at<N, ROW>(0, l0 + bl_off, pt)], x1 = W[hd_at<N, ROW>(1, l0 + bl_off, pt)];
-        hd_mma(c0, a, bri ? x0.y : x0.x);
-        hd_mma(c1, a, bri ? x1.y : x1.x);
+        const double2 x0 = W[hd_at<N, ROW>(0, l0 + (lane >> 2), pt)];
+        const double2 x1 = W[hd_at<N, ROW>(1, l0 + (lane >> 2), pt)];
+        hd_mma(acc[0], a, x0.x);
+        hd_mma(acc[1], a, x0.y);
+        hd_mma(acc[2], a, x1.x);
+        hd_mma(acc[3], a, x1.y);
       }
-      const double sg = ((j & 1) ? -nq : nq) * bbar[line];
-      const double2 r0 = o0[ti] + make_double2(c0[0], c0[1]) + sg * alt[line];
-      const double2 r1 = o1[ti] + make_double2(c1[0], c1[1]) + sg * alt[N + line];
-      emit(line, j, g, r0, r1, pv);
+      const double nqj = (j & 1) ? -nq : nq;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int line = lp + u;
+        const double sg = nqj * bbar[line];
+        const double2 r0 = o[ti][u][0] + make_double2(acc[0][u], acc[1][u]) + sg * alt[line];
+        const double2 r1 = o[ti][u][1] + make_double2(acc[2][u], acc[3][u]) + sg * alt[N + line];
+        emit(line, j, u == 0 ? g0 : g1, r0, r1, u == 0 ? pv0 : pv1);
+      }
     }
   }
   __syncthreads();
