@@ -132,8 +132,9 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     const char* gk = getenv("HFB_F64_MMA");
     c->f64_mma = (gk && gk[0] == '0') ? 0 : 1;
     // single-precision rotation fed by TMA unless HFB_TMA_FEED=0
+    // FP64 hpsi on the FP64 tensor cores unless HFB_F64_HPSI=fft
     const char* fh = getenv("HFB_F64_HPSI");
-    c->f64_hpsi = (fh && strcmp(fh, "dmma") == 0) ? 1 : 0;
+    c->f64_hpsi = (fh && strcmp(fh, "fft") == 0) ? 0 : 1;
     const char* gt = getenv("HFB_TMA_FEED");
     c->tma_feed = (gt && gt[0] == '0') ? 0 : 1;
     c->wait_limit = kDefaultWaitLimit;

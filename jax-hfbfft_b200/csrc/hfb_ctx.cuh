@@ -28,7 +28,7 @@ struct hfb_ctx_s {
   int hpsi_kind;         // single-precision hpsi kernel: 0 bf16 three-term (default), 1 tf32 three-term, 2 FFT
                          // on CUDA cores (HFB_HPSI_KERNEL=bf16x3 / tf32x3 / fft at creation, hfb_set_hpsi_kernel)
   int f64_mma;           // FP64 Gram and rotation on the FP64 tensor cores (default; HFB_F64_MMA=0: CUDA cores)
-  int f64_hpsi;          // FP64 hpsi: 0 FFT kernels, 1 FP64 tensor cores (HFB_F64_HPSI=fft / dmma at creation)
+  int f64_hpsi;          // FP64 hpsi: 1 FP64 tensor cores (default), 0 FFT kernels (HFB_F64_HPSI=fft at creation)
   double* hpsi_d64;      // FP64 hpsi on the tensor cores: D of each axis, [3][n][n] doubles
   int tma_feed;          // single-precision rotation: K blocks by TMA, A in TMEM (default; HFB_TMA_FEED=0 at
                          // creation: producers that load through registers)

@@ -106,11 +106,12 @@ def test_hpsi_batched_against_oracle(n, dtype, ns):
 
 
 @pytest.mark.parametrize("n,ns", [(8, 3), (16, 5), (24, 5), (40, 5), (48, 5), (48, 9)])
-def test_hpsi_fp64_tensor_cores_against_oracle(monkeypatch, n, ns):
-    """FP64 hpsi on the FP64 tensor cores (HFB_F64_HPSI=dmma at context
-    creation: D as an n x n matrix, mma.sync m8n8k4 .f64) against the oracle,
-    to the same 1e-11 as the FFT kernels."""
-    monkeypatch.setenv("HFB_F64_HPSI", "dmma")
+def test_hpsi_fp64_fft_kernels_against_oracle(monkeypatch, n, ns):
+    """FP64 hpsi by the FFT kernels (HFB_F64_HPSI=fft at context creation;
+    the default is the FP64 tensor-core form, D as an n x n matrix and
+    mma.sync m8n8k4 .f64, which the batched test above checks) against the
+    oracle, to the same 1e-11."""
+    monkeypatch.setenv("HFB_F64_HPSI", "fft")
     _check_hpsi_batched(n, torch.complex128, ns)
 
 
