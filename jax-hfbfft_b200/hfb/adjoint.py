@@ -16,9 +16,12 @@ volume / density-dependent delta pairing (meanfield.py:368-382), a pairing
 energy linear in v0_q: dE/dv0_q = -epair_q / v0_q (pairs.py:116-126, the
 pairing energy enters E_bind with a minus sign, energies.py:313-315).
 
-Parameters (``PARAMS``): t0-t3, x0-x3, W0 (= t4, with b4p scaled in
-proportion, so SLy4's b4 = b4p = W0/2 move together), power (alpha), and
-v0neut, v0prot.
+Parameters (``PARAMS``): the eleven Skyrme couplings of the force table
+(forces.py:60-107) t0-t3, x0-x3, t4 (the spin-orbit strength W0 as it
+enters b4 = t4/2), b4p (the isovector spin-orbit coefficient, independent
+of t4 in the table) and power (alpha), then v0neut, v0prot.  ``W0`` is also
+accepted: the direction that moves t4 and b4p in proportion (SLy4's b4 =
+b4p = W0/2 together), the coupling the parameter sweep perturbs.
 
 ``coupling_gradient(state)`` evaluates the gradient on a converged state;
 ``converge`` runs a state to a tight energy tolerance; ``fd_gradient`` is the
@@ -36,7 +39,8 @@ import torch
 from . import config, static
 from ._lib import call, ptr, stream_ptr, HFB_F64
 
-PARAMS = ("t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power", "v0neut", "v0prot")
+SKYRME = ("t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "t4", "b4p", "power")
+PARAMS = SKYRME + ("v0neut", "v0prot")
 _B = ("b0", "b0p", "b1", "b1p", "b2", "b2p", "b3", "b3p", "b4", "b4p")
 
 
@@ -68,12 +72,15 @@ def _db_dtheta(f):
         "x2": {"b1": t2 / 8.0, "b1p": -t2 / 4.0, "b2": -t2 / 16.0, "b2p": t2 / 8.0},
         "t3": {"b3": (1.0 + 0.5 * x3) / 4.0, "b3p": (0.5 + x3) / 4.0},
         "x3": {"b3": t3 / 8.0, "b3p": t3 / 4.0},
+        "t4": {"b4": 0.5},
+        "b4p": {"b4p": 1.0},
         "W0": {"b4": 0.5, "b4p": (f.b4p / t4) if t4 != 0.0 else 0.0},
     }
 
 
 def coupling_gradient(state):
-    """dE_bind/dtheta for every name in PARAMS on a converged state."""
+    """dE_bind/dtheta for every name in PARAMS (and W0) on a converged
+    state."""
     f = state["forces"]
     gb = b_gradient(state)
     jac = _db_dtheta(f)
@@ -90,7 +97,8 @@ def coupling_gradient(state):
 
 def force_overrides(case, theta):
     """A copy of ``case`` whose force block carries the couplings of
-    ``theta`` (dict name -> value; names from PARAMS, W0 scales b4p)."""
+    ``theta`` (dict name -> value; names from PARAMS, or W0, which scales
+    b4p with t4)."""
     from .forces import FORCE_TABLE
     c = copy.deepcopy(case)
     fb = c["force"]
@@ -112,8 +120,7 @@ def force_overrides(case, theta):
 
 def theta_of(forces):
     """Current values of PARAMS for a Forces object."""
-    t = {k: getattr(forces, k) for k in ("t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "power", "v0neut",
-                                         "v0prot")}
+    t = {k: getattr(forces, k) for k in PARAMS}
     t["W0"] = forces.t4
     return t
 

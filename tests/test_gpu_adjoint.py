@@ -1,7 +1,8 @@
 """Sensitivities (hfb.adjoint) against central finite differences (relative
 step 1e-4) of the self-consistent solution, on the Ca48 sensitivity
 workload (32^3, dx 0.8 fm, 40 + 30 states, SLy4 + volume delta pairing):
-the binding energy's explicit gradient for the ten Skyrme couplings and
+the binding energy's explicit gradient for the eleven Skyrme couplings
+(t0-t3, x0-x3, t4, b4p, alpha) and
 both pairing strengths, and the proton rms radius's gradient by the
 implicit adjoint (linear-response solve at the fixed point).  Ca48 is
 doubly magic: its BCS gap all but collapses, the occupations are within
@@ -27,11 +28,14 @@ def test_coupling_gradient_matches_central_fd(ca48):
     1e-4 relative for the Skyrme couplings."""
     from hfb import adjoint
     case, st = ca48
-    names = ["t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power"]
+    names = list(adjoint.SKYRME)
     g = adjoint.coupling_gradient(st)
     fd = adjoint.fd_gradient(case, names, rel_step=1e-4, base=st, tol=1e-11)
     for n in names:
         assert abs(g[n] - fd[n]) <= 1e-4 * abs(fd[n]), (n, g[n], fd[n])
+    # W0 moves t4 and b4p in proportion: its gradient is the chain rule of the two
+    f = st["forces"]
+    assert abs(g["W0"] - (g["t4"] + f.b4p / f.t4 * g["b4p"])) <= 1e-12 * abs(g["W0"])
 
 
 @pytest.mark.gpu
@@ -51,7 +55,7 @@ def test_pairing_strength_gradient_collapsed_pairing(ca48):
 def test_coupling_gradient_with_bcs_pairing_cr48():
     """Cr48 (32^3, 32 + 32 states, volume-delta pairing with the 60 MeV soft
     window, open shells; a weak BCS solution, epair about 1 keV per
-    isospin): dE_bind/dtheta for the ten Skyrme couplings from the explicit
+    isospin): dE_bind/dtheta for the eleven Skyrme couplings from the explicit
     derivative against central differences (relative step 1e-4) to 1e-4
     relative (measured on B200: at most 5.3e-5).  The pairing strengths are
     left out: there the reference's BCS (soft cutoff, floored u v) is not
@@ -60,7 +64,7 @@ def test_coupling_gradient_with_bcs_pairing_cr48():
     from hfb import config, adjoint
     case = config.case_dict("Cr48")
     st, _ = adjoint.converge(case, tol=1e-11, maxiter=3000)
-    names = ["t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power"]
+    names = list(adjoint.SKYRME)
     g = adjoint.coupling_gradient(st)
     fd = adjoint.fd_gradient(case, names, rel_step=1e-4, base=st, tol=1e-11, maxiter=3000)
     for n in names:
@@ -96,13 +100,13 @@ def ca48_states():
 
 @pytest.mark.gpu
 def test_rms_gradient_implicit_adjoint_matches_central_fd(ca48_states):
-    """dr_rms(p)/dtheta for the ten Skyrme couplings: the adjoint solve
+    """dr_rms(p)/dtheta for the eleven Skyrme couplings: the adjoint solve
     (CG on the occupied-virtual orbital Hessian) against central
     differences of the reconverged radius, 1e-4 relative (measured on B200:
     at most 8.4e-6, CG residual 7e-11 after 79 iterations)."""
     from hfb import adjoint
     case, st = ca48_states
-    names = ["t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "W0", "power"]
+    names = list(adjoint.SKYRME)
     g, info = adjoint.rms_gradient(st, names, tol=1e-9, allow_fractional=True)
     assert info["residual"] < 1e-9 and info["cg_iterations"] < 500
     fd = adjoint.fd_rms_gradient(case, names, rel_step=1e-4, base=st, tol_r=1e-13)
