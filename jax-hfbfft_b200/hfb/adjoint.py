@@ -450,3 +450,46 @@ def fd_rms_gradient(case, names, rel_step=1e-4, base=None, **kw):
             converge_states(force_overrides(case, {name: th0[name] - h}), init_psi=psi0, **kw)[0]))[1][1]
         out[name] = (rp - rm) / (2.0 * h)
     return out
+
+
+def check(case_name="Ca48", rms=True, names=SKYRME, rel_step=1e-4):
+    """The sensitivities of ``case_name`` against central differences of
+    the reconverged solution: {"E": {name: (gradient, fd, rel diff)},
+    "rms": {...}, "cg": {...}}.  The radius part needs integer-like
+    occupations (see RmsResponse); it is skipped with ``rms=False``."""
+    case = config.case_dict(case_name)
+    st, _ = converge(case, tol=1e-11, maxiter=3000)
+    g = coupling_gradient(st)
+    fd = fd_gradient(case, list(names), rel_step=rel_step, base=st, tol=1e-11, maxiter=3000)
+    out = {"E": {n: (g[n], fd[n], abs(g[n] - fd[n]) / abs(fd[n])) for n in names}}
+    if rms:
+        sr, _ = converge_states(case, tol_r=1e-13)
+        gr, info = rms_gradient(sr, list(names), tol=1e-9, allow_fractional=True)
+        fr = fd_rms_gradient(case, list(names), rel_step=rel_step, base=sr, tol_r=1e-13)
+        out["rms"] = {n: (gr[n], fr[n], abs(gr[n] - fr[n]) / abs(fr[n])) for n in names}
+        out["cg"] = {"iterations": int(info["cg_iterations"]), "residual": float(info["residual"])}
+    return out
+
+
+def main(argv=None):
+    """python -m hfb.adjoint [--case Ca48] [--no-rms]: print the check table
+    (gradient, central difference, relative difference per coupling)."""
+    import argparse
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--case", default="Ca48")
+    ap.add_argument("--no-rms", action="store_true")
+    args = ap.parse_args(argv)
+    res = check(args.case, rms=not args.no_rms)
+    for part in ("E", "rms"):
+        if part not in res:
+            continue
+        print(f"d{'E_bind' if part == 'E' else 'r_rms(p)'}/dtheta, {args.case}:")
+        for n, (a, b, r) in res[part].items():
+            print(f"  {n:6s} {a:+.6e} {b:+.6e} {r:.2e}")
+        print(f"  max relative difference {max(v[2] for v in res[part].values()):.2e}")
+    if "cg" in res:
+        print(f"  adjoint CG: {res['cg']['iterations']} iterations, residual {res['cg']['residual']:.1e}")
+
+
+if __name__ == "__main__":
+    main()
