@@ -137,6 +137,9 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     c->f64_hpsi = (fh && strcmp(fh, "fft") == 0) ? 0 : 1;
     const char* gt = getenv("HFB_TMA_FEED");
     c->tma_feed = (gt && gt[0] == '0') ? 0 : 1;
+    // H and G Gram matrices computed while the lambda eigensolve runs unless HFB_GRAM_SPLIT=0
+    const char* gs = getenv("HFB_GRAM_SPLIT");
+    c->gram_split = (gs && gs[0] == '0') ? 0 : 1;
     c->wait_limit = kDefaultWaitLimit;
     c->timeout_probe = 0;
   }

@@ -1769,16 +1769,22 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
   off.v[0] = 0; off.v[1] = n0;
   const int nq[2] = {n0, n1}, so[2] = {0, n0};
   int r;
+  // The eigensolve of lambda runs on the side stream on a few SMs.  H and G
+  // are needed only by the construct step after it, so when both are asked
+  // for, the Gram launch computes S and lambda first and H, G follow on the
+  // main stream while the eigensolve runs (HFB_GRAM_SPLIT=0: one launch).
+  int mask = 1;
+  if (a->diagonalize) mask |= 2;
+  if (a->construct) mask |= 4;
+  if (a->construct && a->ipair) mask |= 8;
+  const bool split = a->diagonalize && a->construct && ctx->side && ctx->gram_split;
+  const double* vp[2] = {a->v_pair, a->v_pair ? a->v_pair + n3 : nullptr};
+  double2* outs[8];
+  for (int iq = 0; iq < 2; ++iq)
+    for (int m = 0; m < 4; ++m) outs[iq * 4 + m] = gm + ((size_t)iq * 4 + m) * sm;
   {
-    int mask = 1;
-    if (a->diagonalize) mask |= 2;
-    if (a->construct) mask |= 4;
-    if (a->construct && a->ipair) mask |= 8;
-    const int masks[2] = {mask, mask};
-    const double* vp[2] = {a->v_pair, a->v_pair ? a->v_pair + n3 : nullptr};
-    double2* outs[8];
-    for (int iq = 0; iq < 2; ++iq)
-      for (int m = 0; m < 4; ++m) outs[iq * 4 + m] = gm + ((size_t)iq * 4 + m) * sm;
+    const int m1 = split ? (mask & 3) : mask;
+    const int masks[2] = {m1, m1};
     r = gram_launch(ctx, prec, 2, so, nq, masks, a->psi, a->hampsi, a->hmfpsi, vp, a->wxyz, outs, ld, st);
     if (r) return r;
   }
@@ -1819,6 +1825,12 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
     }
     if (r) return r;
     if (fork) cudaEventRecord(ctx->ev_join, ctx->side);
+  }
+  if (split) {
+    const int m2 = mask & 12;
+    const int masks[2] = {m2, m2};
+    r = gram_launch(ctx, prec, 2, so, nq, masks, a->psi, a->hampsi, a->hmfpsi, vp, a->wxyz, outs, ld, st);
+    if (r) return r;
   }
   r = loewdin_ns(ctx, ld, nper, gm, 4 * sm, Y0, Z0, Y1, Z1, T, cinv, gate, Ur, st);
   if (r) return r;

@@ -34,6 +34,7 @@ struct hfb_ctx_s {
                          // creation: producers that load through registers)
   long long wait_limit;  // clock cycles any one bounded device wait may take (hfb_set_wait_limit)
   int timeout_probe;     // the next tensor-core hpsi launch runs its timeout path (hfb_arm_timeout_probe)
+  int gram_split;        // diagstep: H, G Gram matrices after the lambda eigensolve's fork (HFB_GRAM_SPLIT)
   // scratch arena: fixed slots, grown on demand (never shrunk)
   enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_HPT, S_LAST, S_NAT, S_RESP, S_RESP2, S_VJP, S_NSLOT };
   void* slot[S_NSLOT];
