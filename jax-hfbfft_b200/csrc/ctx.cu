@@ -166,6 +166,12 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     cudaGetLastError();
     c->side = nullptr;
   }
+  if (cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join2, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    c->side2 = nullptr;
+  }
   const size_t n2c = (size_t)c->n2 * c->n2 * c->n2;
   if (cudaMalloc(&c->coul_q, n2c * sizeof(double2)) != cudaSuccess) {
     hfb_ctx_destroy(c);
@@ -200,6 +206,11 @@ extern "C" int hfb_ctx_destroy(hfb_ctx_t c) {
     cudaStreamDestroy(c->side);
     cudaEventDestroy(c->ev_fork);
     cudaEventDestroy(c->ev_join);
+  }
+  if (c->side2) {
+    cudaStreamDestroy(c->side2);
+    cudaEventDestroy(c->ev_fork2);
+    cudaEventDestroy(c->ev_join2);
   }
   for (int s = 0; s < hfb_ctx_s::S_NSLOT; ++s)
     if (c->slot[s]) cudaFree(c->slot[s]);

@@ -1790,6 +1790,15 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
   }
   diag_real_kernel<<<2, 256, 0, st>>>(ld, nper, off, gm, 4 * sm, a->sp_norm);
   HFB_CHECK_LAUNCH();
+  // Newton-Schulz needs S only: with the split Gram it runs on a second side
+  // stream, beside the H, G launch and the eigensolve, on the SMs they leave
+  const bool ns_side = split && ctx->side2;
+  cudaStream_t nst = st;
+  if (ns_side) {
+    cudaEventRecord(ctx->ev_fork2, st);
+    cudaStreamWaitEvent(ctx->side2, ctx->ev_fork2, 0);
+    nst = ctx->side2;
+  }
   // eigh of lambda (Jacobi, one CTA per isospin) on the side stream while the
   // Newton-Schulz GEMMs for S^-1/2 run on the main stream
   const bool fork = a->diagonalize && ctx->side;
@@ -1832,8 +1841,12 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
     r = gram_launch(ctx, prec, 2, so, nq, masks, a->psi, a->hampsi, a->hmfpsi, vp, a->wxyz, outs, ld, st);
     if (r) return r;
   }
-  r = loewdin_ns(ctx, ld, nper, gm, 4 * sm, Y0, Z0, Y1, Z1, T, cinv, gate, Ur, st);
+  r = loewdin_ns(ctx, ld, nper, gm, 4 * sm, Y0, Z0, Y1, Z1, T, cinv, gate, Ur, nst);
   if (r) return r;
+  if (ns_side) {
+    cudaEventRecord(ctx->ev_join2, ctx->side2);
+    cudaStreamWaitEvent(st, ctx->ev_join2, 0);
+  }
   double2* Uuse = Ur;
   if (a->diagonalize) {
     if (fork) cudaStreamWaitEvent(st, ctx->ev_join, 0);

@@ -23,6 +23,8 @@ struct hfb_ctx_s {
   int lambda_refine;     // FP64 diagstep diagonalises lambda by eigen refinement (default 1;
                          // HFB_LAMBDA_JACOBI=1 at creation selects the Jacobi solver)
   cudaEvent_t ev_fork, ev_join;
+  cudaStream_t side2;    // a second one (Newton-Schulz beside the eigensolve and the H, G Gram)
+  cudaEvent_t ev_fork2, ev_join2;
   unsigned char* hpsi_b; // single-precision hpsi (tf32 kernel): derivative matrices in the tensor-core tile layout
   unsigned char* hpsi_bf3_b; // single-precision hpsi (bf16 three-term kernel): the same, bf16 h/m/l tiles
   int hpsi_kind;         // single-precision hpsi kernel: 0 bf16 three-term (default), 1 tf32 three-term, 2 FFT
