@@ -1659,15 +1659,18 @@ rotate_f32_kernel(int ns, size_t K, const float2* __restrict__ psi, const double
 }
 
 int rotate_tc_launch(hfb_ctx_s* c, int ns, const void* psi, const double2* U, const double2* L, int ld, void* out1,
-                     void* out2, cudaStream_t st);   // rotate_tc.cu
+                     void* out2, cudaStream_t st, int pre);   // rotate_tc.cu
+int rotate_tc_transpose(hfb_ctx_s* c, int which, int ns, const void* psi, cudaStream_t st);
 
+// ``pre`` (single precision on the tensor cores): 0 or 1 when the states were
+// transposed already by rotate_tc_transpose into that rotation's buffer.
 int rotate_launch(hfb_ctx_s* c, int prec, int s0, int ns, const void* psi, const double2* U, const double2* L, int ld,
-                  void* out1, void* out2, cudaStream_t st) {
+                  void* out1, void* out2, cudaStream_t st, int pre) {
   if (ns <= 0) return HFB_OK;
   if (prec != HFB_F64 && c->use_tcgen05) {
     const size_t Kc = (size_t)2 * c->n * c->n * c->n, offc = (size_t)s0 * Kc;
     const int r = rotate_tc_launch(c, ns, (const float2*)psi + offc, U, L, ld, (float2*)out1 + offc,
-                                   (float2*)out2 + offc, st);
+                                   (float2*)out2 + offc, st, pre);
     if (r != HFB_ERR_UNSUPPORTED_GRID) return r;
   }
   const size_t K = (size_t)2 * c->n * c->n * c->n;
@@ -1843,6 +1846,17 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
   }
   r = loewdin_ns(ctx, ld, nper, gm, 4 * sm, Y0, Z0, Y1, Z1, T, cinv, gate, Ur, nst);
   if (r) return r;
+  // the rotation's transposes of the states depend on psi only: they follow
+  // Newton-Schulz on the second side stream
+  int pre[2] = {-1, -1};
+  if (ns_side && prec != HFB_F64 && ctx->use_tcgen05) {
+    const size_t Kc = (size_t)2 * n3;
+    for (int iq = 0; iq < 2; ++iq) {
+      r = rotate_tc_transpose(ctx, iq, nq[iq], (const float2*)a->psi + (size_t)so[iq] * Kc, nst);
+      if (r == HFB_OK) pre[iq] = iq;
+      else if (r != HFB_ERR_UNSUPPORTED_GRID) return r;
+    }
+  }
   if (ns_side) {
     cudaEventRecord(ctx->ev_join2, ctx->side2);
     cudaStreamWaitEvent(st, ctx->ev_join2, 0);
@@ -1879,7 +1893,7 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
   if (r) return r;
   for (int iq = 0; iq < 2; ++iq) {
     r = rotate_launch(ctx, prec, so[iq], nq[iq], a->psi, Uuse + (size_t)iq * sm, Lw + (size_t)iq * sm, ld, a->psi_out,
-                      a->lagrange, st);
+                      a->lagrange, st, pre[iq]);
     if (r) return r;
   }
   return HFB_OK;

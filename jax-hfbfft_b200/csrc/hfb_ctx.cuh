@@ -38,7 +38,7 @@ struct hfb_ctx_s {
   int timeout_probe;     // the next tensor-core hpsi launch runs its timeout path (hfb_arm_timeout_probe)
   int gram_split;        // diagstep: H, G Gram matrices after the lambda eigensolve's fork (HFB_GRAM_SPLIT)
   // scratch arena: fixed slots, grown on demand (never shrunk)
-  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_HPT, S_LAST, S_NAT, S_RESP, S_RESP2, S_VJP, S_NSLOT };
+  enum { S_PART = 0, S_PART2, S_POIS, S_DENS, S_DERIV, S_GRAM, S_MAT, S_SMALL, S_RED, S_EIG, S_ROT, S_HPT, S_LAST, S_NAT, S_RESP, S_RESP2, S_VJP, S_ROT2, S_NSLOT };
   void* slot[S_NSLOT];
   size_t slot_bytes[S_NSLOT];
 };

@@ -35,7 +35,7 @@ namespace hfb {
 int zgemm_small_one(int n, int ld, int ta, int tb, const double2* A, const double2* B, double2* C,
                     cudaStream_t st);   // diag.cu
 int rotate_launch(hfb_ctx_s* c, int prec, int s0, int ns, const void* psi, const double2* U, const double2* L, int ld,
-                  void* out1, void* out2, cudaStream_t st);   // diag.cu
+                  void* out1, void* out2, cudaStream_t st, int pre);   // diag.cu
 
 namespace {
 
@@ -347,7 +347,7 @@ extern "C" int hfb_natural_end(hfb_ctx_t ctx, int prec, const hfb_natural_args* 
   const int n = a->nst, nn = n * n, s = a->start;
   // [psi cm | psi (cm htran)] for the block's states
   if ((r = zgemm_small_one(n, n, 0, 0, w.cm, w.ht, w.cml, st))) return r;
-  if ((r = rotate_launch(ctx, prec, s, n, psi, w.cm, w.cml, n, psi_out, lagrange, st))) return r;
+  if ((r = rotate_launch(ctx, prec, s, n, psi, w.cm, w.cml, n, psi_out, lagrange, st, -1))) return r;
   nat_store_kernel<<<(nn + 255) / 256, 256, 0, st>>>(n, a->ld, w.ht, matw(a->hmatrix, a));
   HFB_CHECK_LAUNCH();
   nat_store_kernel<<<(nn + 255) / 256, 256, 0, st>>>(n, a->ld, w.gt, matw(a->gapmatrix, a));

@@ -475,31 +475,63 @@ rotate_tma_kernel(RtJob job, const __grid_constant__ CUtensorMap mpt, const unsi
 
 }  // namespace
 
-// out1 = psi U, out2 = psi L for ns complex64 states at psi (offset already
-// applied).  HFB_ERR_UNSUPPORTED_GRID when the grid's 2 n^3 is not a
-// multiple of 128 (the caller then uses the CUDA-core kernel).
-int rotate_tc_launch(hfb_ctx_s* c, int ns, const void* psi, const double2* U, const double2* L, int ld, void* out1,
-                     void* out2, cudaStream_t st) {
-  if (ns <= 0) return HFB_OK;
-  const size_t K = (size_t)2 * c->n * c->n * c->n;
-  if (K % 128 != 0) return HFB_ERR_UNSUPPORTED_GRID;
+static RtJob rt_job(hfb_ctx_s* c, int ns) {
   RtJob job{};
-  job.K = K;
+  job.K = (size_t)2 * c->n * c->n * c->n;
   job.ns = ns;
   job.ldT = (ns + 15) / 16 * 16;
   job.nkb = job.ldT / 16;
   job.nchunk = (4 * ns + kRtN - 1) / kRtN;
-  job.ntile = (int)(K / 128);
+  job.ntile = (int)(job.K / 128);
   job.ntask = job.ntile * job.nchunk;
-  const size_t tbytes = sizeof(float2) * K * (size_t)job.ldT;
+  return job;
+}
+
+// The job's buffer (psiT, then the B tiles) in scratch slot ``slot``.
+static unsigned char* rt_buffer(hfb_ctx_s* c, const RtJob& job, int slot, size_t* tbytes) {
+  *tbytes = sizeof(float2) * job.K * (size_t)job.ldT;
   const size_t bbytes = (size_t)job.nchunk * job.nkb * 2 * kRtBBytes;
-  unsigned char* buf = (unsigned char*)scratch(c, hfb_ctx_s::S_ROT, tbytes + bbytes + 1024);
+  return (unsigned char*)scratch(c, slot, *tbytes + bbytes + 1024);
+}
+
+// psiT (the K-major A operand) of ns complex64 states at psi, into the
+// buffer of rotation ``which`` (0 or 1): the transpose depends on psi only,
+// so the diagonalisation step issues it early, beside the Gram and the
+// eigensolve.  HFB_ERR_UNSUPPORTED_GRID as rotate_tc_launch.
+int rotate_tc_transpose(hfb_ctx_s* c, int which, int ns, const void* psi, cudaStream_t st) {
+  if (ns <= 0) return HFB_OK;
+  const RtJob job = rt_job(c, ns);
+  if (job.K % 128 != 0) return HFB_ERR_UNSUPPORTED_GRID;
+  size_t tbytes;
+  unsigned char* buf = rt_buffer(c, job, which ? hfb_ctx_s::S_ROT2 : hfb_ctx_s::S_ROT, &tbytes);
+  if (!buf) return HFB_ERR_ALLOC;
+  dim3 tg((unsigned)((job.K + 31) / 32), (unsigned)((job.ldT + 31) / 32));
+  psi_transpose_kernel<<<tg, dim3(32, 8), 0, st>>>((const float2*)psi, (float2*)buf, ns, job.ldT, job.K);
+  HFB_CHECK_LAUNCH();
+  return HFB_OK;
+}
+
+// out1 = psi U, out2 = psi L for ns complex64 states at psi (offset already
+// applied).  ``pre`` = 0 or 1: psiT is already in the buffer of that
+// rotation (rotate_tc_transpose on the same states); -1: transposed here.
+// HFB_ERR_UNSUPPORTED_GRID when the grid's 2 n^3 is not a multiple of 128
+// (the caller then uses the CUDA-core kernel).
+int rotate_tc_launch(hfb_ctx_s* c, int ns, const void* psi, const double2* U, const double2* L, int ld, void* out1,
+                     void* out2, cudaStream_t st, int pre) {
+  if (ns <= 0) return HFB_OK;
+  const RtJob job = rt_job(c, ns);
+  const size_t K = job.K;
+  if (K % 128 != 0) return HFB_ERR_UNSUPPORTED_GRID;
+  size_t tbytes;
+  unsigned char* buf = rt_buffer(c, job, pre == 1 ? hfb_ctx_s::S_ROT2 : hfb_ctx_s::S_ROT, &tbytes);
   if (!buf) return HFB_ERR_ALLOC;
   float2* psiT = (float2*)buf;
   unsigned char* bt = buf + ((tbytes + 1023) / 1024) * 1024;
-  dim3 tg((unsigned)((K + 31) / 32), (unsigned)((job.ldT + 31) / 32));
-  psi_transpose_kernel<<<tg, dim3(32, 8), 0, st>>>((const float2*)psi, psiT, ns, job.ldT, K);
-  HFB_CHECK_LAUNCH();
+  if (pre < 0) {
+    dim3 tg((unsigned)((K + 31) / 32), (unsigned)((job.ldT + 31) / 32));
+    psi_transpose_kernel<<<tg, dim3(32, 8), 0, st>>>((const float2*)psi, psiT, ns, job.ldT, K);
+    HFB_CHECK_LAUNCH();
+  }
   const int nprep = job.nchunk * job.nkb * kRtN * 8;
   rot_b_prep_kernel<<<(nprep + 255) / 256, 256, 0, st>>>(U, L, ld, ns, job.nkb, job.nchunk, bt);
   HFB_CHECK_LAUNCH();

@@ -457,9 +457,22 @@ extern "C" int hfb_skyrme(hfb_ctx_t ctx, const hfb_force* f, int tcoul, const do
   cudaStream_t st = as_stream(stream);
   const size_t n3 = (size_t)ctx->n * ctx->n * ctx->n;
   double* dv = nullptr;
-  int r = density_derivatives(ctx, rho, current, sdens, sodens, true, &dv, st);
+  // the Coulomb solve needs rho_p only: on the side stream, beside the
+  // derivatives of the densities
+  const bool fork = tcoul && ctx->side;
+  int r;
+  if (fork) {
+    cudaEventRecord(ctx->ev_fork, st);
+    cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
+    r = poisson_launch(ctx, rho + n3, wcoul, ctx->side);
+    if (r) return r;
+    cudaEventRecord(ctx->ev_join, ctx->side);
+  }
+  r = density_derivatives(ctx, rho, current, sdens, sodens, true, &dv, st);
   if (r) return r;
-  if (tcoul) {
+  if (fork) {
+    cudaStreamWaitEvent(st, ctx->ev_join, 0);
+  } else if (tcoul) {
     r = poisson_launch(ctx, rho + n3, wcoul, st);
     if (r) return r;
   }
