@@ -460,6 +460,46 @@ def test_rotation_tma_feed_matches_register_producers(monkeypatch):
     assert np.max(np.abs(e1 - e2)) < 1e-3
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64], ids=["f64", "f32"])
+def test_diagstep_overlapped_matches_sequential(monkeypatch, dtype):
+    """The diagonalisation step with the H, G Gram launch, Newton-Schulz and
+    the rotation's transposes overlapping the lambda eigensolve on side
+    streams (the default) against the same step with one Gram launch and
+    everything after it on the main stream (HFB_GRAM_SPLIT=0 at context
+    creation), on Pb208 after two iterations: the FP64 Gram's tiles do not
+    depend on the matrices computed with it, so FP64 agrees bit for bit;
+    single precision to its rounding (the tensor-core Gram's K slices are
+    shared out by the number of matrices in the launch)."""
+    from hfb import config, static
+
+    def run():
+        st = config.setup(config.case_dict("Pb208"), dtype=torch.complex128)
+        S = {k: st[k] for k in static._STATE_KEYS}
+        static.prepare(**S)
+        for i in (1, 2):
+            static.iterate(i, **S)
+        if dtype != torch.complex128:
+            static.to_precision(st, dtype)
+        static.diagstep(st["energies"], st["forces"], st["grids"], st["levels"], st["static"], True, True)
+        torch.cuda.synchronize()
+        st["grids"].ctx.check("diagstep")
+        lv = st["levels"]
+        return (lv.psi.detach().clone(), lv.lagrange.detach().clone(), lv.sp_energy.detach().cpu().numpy().copy(),
+                st["static"].hmatrix.detach().cpu().numpy().copy())
+
+    p1, l1, e1, h1 = run()
+    monkeypatch.setenv("HFB_GRAM_SPLIT", "0")
+    p2, l2, e2, h2 = run()
+    if dtype == torch.complex128:
+        assert torch.equal(p1, p2) and torch.equal(l1, l2)
+        assert np.array_equal(e1, e2) and np.array_equal(h1, h2)
+    else:
+        assert float((p1 - p2).abs().max()) <= 1e-4 * float(p2.abs().max())
+        assert float((l1 - l2).abs().max()) <= 1e-4 * float(l2.abs().max())
+        assert np.max(np.abs(e1 - e2)) < 1e-3
+
+
 def _near_diag_hermitian(n, seed, scale, kramers=True):
     """Hermitian test matrix close to diagonal: spread diagonal with exactly
     degenerate pairs (as time reversal gives), plus a random Hermitian
