@@ -468,9 +468,13 @@ def test_diagstep_overlapped_matches_sequential(monkeypatch, dtype):
     streams (the default) against the same step with one Gram launch and
     everything after it on the main stream (HFB_GRAM_SPLIT=0 at context
     creation), on Pb208 after two iterations: the FP64 Gram's tiles do not
-    depend on the matrices computed with it, so FP64 agrees bit for bit;
-    single precision to its rounding (the tensor-core Gram's K slices are
-    shared out by the number of matrices in the launch)."""
+    depend on the matrices computed with it, so FP64 agrees bit for bit.
+    In single precision the tensor-core Gram's K slices are shared out by
+    the number of matrices in the launch, so lambda differs at rounding
+    level and the eigensolver picks another basis inside the degenerate
+    (Kramers) pairs: the checks are gauge invariant -- each state of one
+    run lies in the span of the other's (row norms of the overlap matrix
+    per isospin) and the sorted single-particle energies agree."""
     from hfb import config, static
 
     def run():
@@ -485,6 +489,7 @@ def test_diagstep_overlapped_matches_sequential(monkeypatch, dtype):
         torch.cuda.synchronize()
         st["grids"].ctx.check("diagstep")
         lv = st["levels"]
+        run.geo = (st["grids"].wxyz, lv.npsi[0], lv.nstmax)
         return (lv.psi.detach().clone(), lv.lagrange.detach().clone(), lv.sp_energy.detach().cpu().numpy().copy(),
                 st["static"].hmatrix.detach().cpu().numpy().copy())
 
@@ -495,9 +500,16 @@ def test_diagstep_overlapped_matches_sequential(monkeypatch, dtype):
         assert torch.equal(p1, p2) and torch.equal(l1, l2)
         assert np.array_equal(e1, e2) and np.array_equal(h1, h2)
     else:
-        assert float((p1 - p2).abs().max()) <= 1e-4 * float(p2.abs().max())
-        assert float((l1 - l2).abs().max()) <= 1e-4 * float(l2.abs().max())
-        assert np.max(np.abs(e1 - e2)) < 1e-3
+        wxyz, n0, ns = run.geo
+        for sl in (slice(0, n0), slice(n0, ns)):
+            a = p1[sl].reshape(sl.stop - sl.start, -1).to(torch.complex128)
+            b = p2[sl].reshape(sl.stop - sl.start, -1).to(torch.complex128)
+            rows = (((a.conj() @ b.T) * wxyz).abs() ** 2).sum(dim=1)
+            assert float((rows - 1).abs().max()) < 2e-5
+        # <psi|h|psi> from complex64 states carries a few keV of rounding at
+        # this stage (measured 6.4e-3 MeV between the two forms), the bound
+        # of the single- against double-precision test above
+        assert np.max(np.abs(np.sort(e1) - np.sort(e2))) < 2e-2
 
 
 def _near_diag_hermitian(n, seed, scale, kramers=True):
