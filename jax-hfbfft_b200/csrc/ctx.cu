@@ -166,11 +166,18 @@ extern "C" int hfb_ctx_create(int nx, int ny, int nz, double dx, double dy, doub
     cudaGetLastError();
     c->side = nullptr;
   }
+  // the second side stream is optional: without it Newton-Schulz stays on
+  // the calling stream
+  c->side2 = nullptr;
+  c->ev_fork2 = c->ev_join2 = nullptr;
   if (cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_join2, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
+    if (c->ev_fork2) cudaEventDestroy(c->ev_fork2);
+    if (c->side2) cudaStreamDestroy(c->side2);
     c->side2 = nullptr;
+    c->ev_fork2 = c->ev_join2 = nullptr;
   }
   const size_t n2c = (size_t)c->n2 * c->n2 * c->n2;
   if (cudaMalloc(&c->coul_q, n2c * sizeof(double2)) != cudaSuccess) {

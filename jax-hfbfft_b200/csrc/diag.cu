@@ -1802,8 +1802,9 @@ extern "C" int hfb_diagstep(hfb_ctx_t ctx, int prec, const hfb_diag_args* a, voi
     cudaStreamWaitEvent(ctx->side2, ctx->ev_fork2, 0);
     nst = ctx->side2;
   }
-  // eigh of lambda (Jacobi, one CTA per isospin) on the side stream while the
-  // Newton-Schulz GEMMs for S^-1/2 run on the main stream
+  // eigh of lambda (Jacobi, one CTA per isospin, or the refinement) on the
+  // side stream while the main stream runs the H, G Gram launch (or, without
+  // the split, the Newton-Schulz GEMMs for S^-1/2)
   const bool fork = a->diagonalize && ctx->side;
   if (a->diagonalize) {
     cudaStream_t es = st;
