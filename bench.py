@@ -220,7 +220,7 @@ def fp64_run(case_name, maxiter):
     return dict(E=E, t=t, e_ref=e_ref, converged=converged, iters=len(E), state=st)
 
 
-def mixed_e2e_run(case_name, maxiter, switch_mev=2e-4):
+def mixed_e2e_run(case_name, maxiter, switch_mev=1e-3):
     """Mixed run through hfb.static.statichf_mixed.  The initial states are
     copied from pinned host memory inside the timed region; E_bind, the
     densities and the single-particle energies are read back at the end."""
@@ -422,7 +422,7 @@ def main():
     ap.add_argument("--cpu-full", action="store_true",
                     help="reference arm: run the oracle to convergence (a measured CPU time-to-converge; small "
                          "workloads only)")
-    ap.add_argument("--switch-mev", type=float, default=2e-4,
+    ap.add_argument("--switch-mev", type=float, default=1e-3,
                     help="mixed run: estimated remaining change (MeV) at which FP32 hands over to FP64")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

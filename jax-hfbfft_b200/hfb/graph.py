@@ -217,7 +217,7 @@ class BatchGraph:
             self.comp = None
 
 
-def solve(states, switch_mev=2e-4, stop_mev=5e-5, floor_mev=5e-5, maxiter=4000, block=10, graph_min=60,
+def solve(states, switch_mev=1e-3, stop_mev=5e-5, floor_mev=5e-5, maxiter=4000, block=10, graph_min=60,
           on_block=None, tune=True, fp32_min_points=static.FP32_MIN_POINTS):
     """Mixed-precision solves of several instances (states with complex64
     psi from hfb.config.setup) advanced together: ordinary iterations

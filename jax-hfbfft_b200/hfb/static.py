@@ -428,11 +428,14 @@ _STATE_KEYS = ("coulomb", "densities", "energies", "forces", "grids", "levels", 
 FP32_MIN_POINTS = 1 << 20
 
 
-def statichf_mixed(state, maxiter=4000, switch_mev=2e-4, floor_mev=5e-5, stop_mev=5e-5, min_tail=3,
+def statichf_mixed(state, maxiter=4000, switch_mev=1e-3, floor_mev=5e-5, stop_mev=5e-5, min_tail=3,
                    on_iteration=None, fp32_min_points=FP32_MIN_POINTS):
     """Mixed-precision self-consistent loop on a state dict from
     hfb.config.setup (states complex64 at entry): FP32 bulk iterations until
-    the estimated remaining energy change is below ``switch_mev`` (or the
+    the estimated remaining energy change is below ``switch_mev`` (default
+    1 keV, the bar of the time-to-converge; measured on Pb208: 6.80 s to
+    within 1 keV against 6.97 s with 0.5 keV and 7.09 s with 0.2 keV, the
+    converged states alike to 2e-5 MeV) (or the
     last 25 energy changes stay below the FP32 noise floor ``floor_mev``),
     then FP64 refinement until the estimated remaining change is below
     ``stop_mev``.  Problems with fewer than ``fp32_min_points`` states times
