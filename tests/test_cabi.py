@@ -184,3 +184,29 @@ def test_observables_layout_matches_header():
         assert enum[names[k]] == off, k
         used[off:off + int(np.prod(shp)) if shp else off + 1] += 1
     assert np.all(used == 1)
+
+
+def test_sensitivity_parameters_and_rebuilt_forces():
+    """The eleven Skyrme couplings of the force table and the two pairing
+    strengths are the sensitivity parameters; W0 is the direction that moves
+    t4 and b4p in proportion (its row is the chain rule of theirs); the
+    forces the response solve rebuilds for one changed coupling equal the
+    table's forces with that override."""
+    from hfb import adjoint
+    from hfb.forces import init_forces
+    assert adjoint.SKYRME == ("t0", "t1", "t2", "t3", "x0", "x1", "x2", "x3", "t4", "b4p", "power")
+    assert adjoint.PARAMS == adjoint.SKYRME + ("v0neut", "v0prot")
+    base = init_forces(None, name="SLy4", ipair=5)
+    th = adjoint.theta_of(base)
+    assert set(adjoint.PARAMS) <= set(th) and th["W0"] == th["t4"]
+    jac = adjoint._db_dtheta(base)
+    for b in ("b4", "b4p"):
+        w0 = jac["t4"].get(b, 0.0) + base.b4p / base.t4 * jac["b4p"].get(b, 0.0)
+        assert jac["W0"].get(b, 0.0) == pytest.approx(w0, rel=1e-15)
+    for name in ("t0", "x2", "t4", "b4p", "power", "W0"):
+        v = th[name] * 1.01
+        f1 = adjoint._forces_at(base, name, v)
+        ov = adjoint.force_overrides(dict(force=dict(name="SLy4")), {name: v})["force"]["overrides"]
+        f2 = init_forces(None, name="SLy4", ipair=5, overrides=ov)
+        for b in ("b0", "b0p", "b1", "b1p", "b2", "b2p", "b3", "b3p", "b4", "b4p", "power"):
+            assert getattr(f1, b) == pytest.approx(getattr(f2, b), rel=1e-14), (name, b)
