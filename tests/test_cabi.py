@@ -210,3 +210,44 @@ def test_sensitivity_parameters_and_rebuilt_forces():
         f2 = init_forces(None, name="SLy4", ipair=5, overrides=ov)
         for b in ("b0", "b0p", "b1", "b1p", "b2", "b2p", "b3", "b3p", "b4", "b4p", "power"):
             assert getattr(f1, b) == pytest.approx(getattr(f2, b), rel=1e-14), (name, b)
+
+
+def _prototypes():
+    """name -> list of parameter declarations of every hfb_* prototype in
+    include/hfb.h (comments removed, multi-line declarations joined)."""
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", " ", txt, flags=re.S)
+    txt = re.sub(r"//[^\n]*", " ", txt)
+    out = {}
+    for m in re.finditer(r"(?:int|const char\*|unsigned long long)\s+(hfb_\w+)\s*\(([^;{]*?)\)\s*;", txt, re.S):
+        params = " ".join(m.group(2).split())
+        out[m.group(1)] = [] if params in ("", "void") else [p.strip() for p in params.split(",")]
+    return out
+
+
+def test_python_prototypes_match_the_header():
+    """Every prototype the Python mirror declares has the header's number of
+    parameters, and each parameter is of the same kind: a pointer for a
+    pointer (device buffer, handle, stream, struct), double for double,
+    long long for long long, int for int."""
+    import ctypes as C
+    from hfb import _lib
+    protos = _prototypes()
+    assert set(_lib._PROTOS) <= set(protos)
+    for name, args in _lib._PROTOS.items():
+        params = protos[name]
+        assert len(params) == len(args), (name, params, args)
+        for p, a in zip(params, args):
+            if "*" in p or p.startswith(("hfb_ctx_t", "void* ")):
+                kind = "ptr"
+            elif p.startswith("double"):
+                kind = "double"
+            elif p.startswith("long long"):
+                kind = "longlong"
+            else:
+                assert p.startswith("int"), (name, p)
+                kind = "int"
+            is_ptr = a is C.c_void_p or (isinstance(a, type) and issubclass(a, C._Pointer))
+            py = ("ptr" if is_ptr else "double" if a is C.c_double else "longlong" if a is C.c_longlong
+                  else "int" if a is C.c_int else repr(a))
+            assert py == kind, (name, p, a)
